@@ -1,0 +1,22 @@
+"""B200-native forward renderer for foveated hybrid-transparency Gaussian splatting.
+
+Drop-in for the rasterization path of TrueKuehli/FoveatedHTGSCudaBackend: the same
+`FoveatedHTGSRasterizer` / `RasterizerSettings` surface and the same positional `_C`,
+`_C_benchmarking` and `_C_stereo` entry points, backed by libfhtgs.so (hand-written sm_100a
+kernels behind the C ABI in include/fhtgs.h).
+"""
+from .rasterization import (  # noqa: F401
+    BackgroundModel,
+    FoveatedHTGSRasterizer,
+    GazeVisualizationType,
+    RasterizerSettings,
+    Renderer,
+    _C,
+    _C_benchmarking,
+    _C_stereo,
+)
+from ._lib import FhtgsError  # noqa: F401
+from .torch_scene import gaussians_to_torch, settings_from_view  # noqa: F401
+
+__all__ = ["FoveatedHTGSRasterizer", "RasterizerSettings", "BackgroundModel", "Renderer", "FhtgsError",
+           "gaussians_to_torch", "settings_from_view"]

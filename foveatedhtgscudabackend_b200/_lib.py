@@ -1,0 +1,143 @@
+"""ctypes binding of libfhtgs.so (include/fhtgs.h).
+
+The shared library is built in-tree by `foveatedhtgscudabackend_b200.build` (nvcc, sm_100a).
+There is no fallback: if the library is missing or fails to load, every render call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libfhtgs.so")
+
+c_f = C.c_float
+c_i32 = C.c_int32
+fp = C.POINTER(C.c_float)
+u32p = C.POINTER(C.c_uint32)
+u16p = C.POINTER(C.c_uint16)
+u8p = C.POINTER(C.c_uint8)
+vp = C.c_void_p
+
+N_STAGES = 8
+STAGE_NAMES = ["setup_classify", "preprocess", "scan_create", "sort", "ranges", "blend_full", "blend_periphery",
+               "compose"]
+
+STATUS = {
+    0: "FHTGS_OK",
+    1: "FHTGS_ERR_INVALID_ARGUMENT",
+    2: "FHTGS_ERR_CUDA",
+    3: "FHTGS_ERR_OUT_OF_MEMORY",
+    4: "FHTGS_ERR_CAPACITY",
+    5: "FHTGS_ERR_NOT_READY",
+}
+
+
+class FhtgsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class Primitives(C.Structure):
+    _fields_ = [("positions", vp), ("scales", vp), ("rotations", vp), ("opacities", vp), ("sh_0", vp),
+                ("sh_rest", vp), ("n_primitives", c_i32), ("total_sh_bases", c_i32)]
+
+
+class View(C.Structure):
+    _fields_ = [("M", vp), ("VPM", vp), ("VPR_inv", vp), ("cam_position", vp), ("gaze_x", c_f), ("gaze_y", c_f),
+                ("visibility_mask", vp), ("visibility_mask_area_table", vp), ("fovea_mask_area_table", vp),
+                ("width", c_i32), ("height", c_i32), ("focal_x", c_f), ("focal_y", c_f), ("center_x", c_f),
+                ("center_y", c_f), ("image", vp)]
+
+
+class Settings(C.Structure):
+    _fields_ = [("K", c_i32), ("active_sh_bases", c_i32), ("near_plane", c_f), ("far_plane", c_f),
+                ("scale_modifier", c_f), ("to_chw", c_i32), ("blur_periphery", c_i32), ("anti_aliasing", c_i32),
+                ("background_type", c_i32), ("background_data", vp), ("texture_width", c_i32),
+                ("texture_height", c_i32), ("fast_math", c_i32)]
+
+
+class FrameInfo(C.Structure):
+    _fields_ = [("n_instances", C.c_int64), ("instance_capacity", C.c_int64), ("n_active_tiles", C.c_uint32),
+                ("partition_ranges", C.c_uint32 * 6), ("overflow", c_i32), ("end_bit", c_i32)]
+
+
+class Intermediates(C.Structure):
+    _fields_ = [("n_touched", u32p), ("screen_bounds", u16p), ("vpmt", fp), ("rgba", fp),
+                ("tile_index_map_partitioned", u32p), ("tile_type_partitioned", u8p), ("keys", u32p),
+                ("values", u32p), ("instance_ranges", u32p)]
+
+
+# Exported symbols and their signatures (mirrors include/fhtgs.h).
+_MONO_ARGS = [vp, vp, vp, vp, vp, vp, vp, c_i32, c_i32, vp, vp, vp, vp, c_f, c_f, vp, vp, vp, vp, c_i32, c_i32,
+              c_i32, c_i32, c_i32, c_i32, c_i32, c_f, c_f, c_f, c_f, c_f, c_f, c_f, c_i32, c_i32, c_i32, vp, vp]
+_STEREO_ARGS = ([vp, vp, vp, vp, vp, vp, vp, c_i32, c_i32]
+                + [vp, vp, vp, vp, c_f, c_f, vp, vp, vp, vp, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32,
+                   c_f, c_f, c_f, c_f, c_f, c_f, c_f]
+                + [vp, vp, vp, vp, c_f, c_f, vp, vp, vp, c_i32, c_i32, c_f, c_f, c_f, c_f]
+                + [c_i32, c_i32, c_i32, vp, vp, vp])
+SIGNATURES = {
+    "fhtgs_abi_version": ([], c_i32),
+    "fhtgs_last_error": ([], C.c_char_p),
+    "fhtgs_context_create": ([c_i32, C.POINTER(vp)], c_i32),
+    "fhtgs_context_destroy": ([vp], c_i32),
+    "fhtgs_context_reserve": ([vp, c_i32, c_i32, c_i32, c_i32, C.c_int64], c_i32),
+    "fhtgs_context_arena_bytes": ([vp], C.c_size_t),
+    "fhtgs_context_launch_count": ([vp], C.c_int64),
+    "fhtgs_context_set_profiling": ([vp, c_i32], c_i32),
+    "fhtgs_get_stage_times": ([vp, C.POINTER(C.c_float), c_i32], c_i32),
+    "fhtgs_get_stage_history": ([vp, C.POINTER(C.c_float), c_i32, C.POINTER(c_i32)], c_i32),
+    "fhtgs_render_views": ([vp, C.POINTER(Primitives), C.POINTER(View), c_i32, C.POINTER(Settings), vp], c_i32),
+    "fhtgs_render_views_sync": ([vp, C.POINTER(Primitives), C.POINTER(View), c_i32, C.POINTER(Settings), vp], c_i32),
+    "fhtgs_get_frame_info": ([vp, c_i32, C.POINTER(FrameInfo)], c_i32),
+    "fhtgs_copy_intermediates": ([vp, c_i32, C.POINTER(Intermediates)], c_i32),
+    "fhtgs_render_mono": (_MONO_ARGS, c_i32),
+    "fhtgs_benchmark_mono": (_MONO_ARGS, c_i32),
+    "fhtgs_render_stereo": (_STEREO_ARGS, c_i32),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load(path: str | None = None) -> C.CDLL:
+    """Loads libfhtgs.so and declares every entry point; raises if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is not None and path is None:
+            return _lib
+        p = path or LIB_PATH
+        if not os.path.exists(p):
+            raise FhtgsError(2, f"{p} is missing; build it with `python -m foveatedhtgscudabackend_b200.build`")
+        lib = C.CDLL(p)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        if path is None:
+            _lib = lib
+        return lib
+
+
+def check(status: int) -> None:
+    if status != 0:
+        msg = load().fhtgs_last_error()
+        raise FhtgsError(status, msg.decode() if msg else "")
+
+
+_contexts: dict[int, int] = {}
+
+
+def context(device: int) -> int:
+    """Process-wide context per CUDA device (owns the device arena)."""
+    with _lock:
+        h = _contexts.get(device)
+    if h is None:
+        out = vp()
+        check(load().fhtgs_context_create(device, C.byref(out)))
+        with _lock:
+            _contexts[device] = out.value
+            h = out.value
+    return h

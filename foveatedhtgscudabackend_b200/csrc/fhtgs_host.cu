@@ -1,0 +1,637 @@
+// Host side of libfhtgs: context with a growable device arena, frame orchestration (all
+// views of a frame in the same launches, no device->host round trip inside a frame) and the
+// C ABI declared in include/fhtgs.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fhtgs.h"
+#include "fhtgs_types.cuh"
+
+using namespace fhtgs;
+
+namespace {
+
+thread_local std::string g_error;
+
+fhtgs_status fail(fhtgs_status code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+#define FHTGS_CK(call)                                                                                     \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) return fail(FHTGS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr size_t kAlign = 256;
+size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+int end_bit_of(uint32_t n) {
+    int b = 0;
+    while (n) { ++b; n >>= 1; }
+    return b;
+}
+
+struct ViewGeom {
+    int glw, glh, n_large, n_tiles, end_bit;
+    int gaze_tx, gaze_ty;
+    float gaze_px, gaze_py;
+};
+
+// Grid sizes, key width and gaze rounding of one view (inference.cu:79-105 of the reference,
+// including its clamp of the gaze tile to the small-tile grid).
+ViewGeom geometry(const fhtgs_view& v) {
+    ViewGeom g;
+    g.glw = (v.width + kTileLarge - 1) / kTileLarge;
+    g.glh = (v.height + kTileLarge - 1) / kTileLarge;
+    g.n_large = g.glw * g.glh;
+    g.n_tiles = g.n_large * kSubTiles;
+    g.end_bit = end_bit_of(static_cast<uint32_t>(g.n_tiles + 1));
+    g.gaze_px = std::min(std::max(v.gaze_x, 0.0f), static_cast<float>(v.width - 1));
+    g.gaze_py = std::min(std::max(v.gaze_y, 0.0f), static_cast<float>(v.height - 1));
+    const int gw = g.glw * kStride, gh = g.glh * kStride;
+    g.gaze_tx = std::max(0, std::min(gw - 1, (static_cast<int>(g.gaze_px) + kTileLarge / 2) / kTileLarge));
+    g.gaze_ty = std::max(0, std::min(gh - 1, (static_cast<int>(g.gaze_py) + kTileLarge / 2) / kTileLarge));
+    return g;
+}
+
+}  // namespace
+
+// Stage boundaries recorded when profiling: start | setup+classify | preprocess |
+// scan+create | sort | ranges | blend full-res | blend periphery | compose.
+constexpr int kStageEvents = 9;
+constexpr int kStageRing = 64;   // frames whose stage events are kept
+
+struct fhtgs_context_s {
+    int device = 0;
+    int n_sms = 148;
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    int64_t cap = 0;              // instance slots per view
+    FrameStatus* h_status = nullptr;  // pinned
+    int h_status_n = 0;
+    // last frame
+    bool have_frame = false;
+    FrameParams fp{};
+    FrameBuffers fb{};
+    std::vector<ViewGeom> geo;
+    std::vector<fhtgs_view> views;
+    cudaStream_t stream = nullptr;
+    // profiling: events around the stages of the last frame, and a launch counter
+    bool profile = false;
+    cudaEvent_t ev[kStageRing][kStageEvents] = {};
+    long long frames_profiled = 0;
+    long long launches = 0;
+};
+
+namespace {
+
+struct Layout {
+    size_t total = 0;
+    size_t off_views, off_status, off_nt, off_bounds, off_rec, off_bsums, off_keys0, off_keys1, off_vals0, off_vals1;
+    size_t off_hist, off_dtot, off_ranges, off_map, off_type, off_ltype, off_wf, off_wl, off_wm, off_ctr, off_temp;
+    std::vector<size_t> temp_offsets;
+};
+
+Layout plan(int V, int64_t N, int nbp, int64_t cap, int key_bytes, int sort_tiles, int max_tiles, int max_large,
+            const std::vector<int64_t>& temp_floats) {
+    Layout L;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { size_t at = o; o = align_up(o + std::max<size_t>(bytes, 1)); return at; };
+    L.off_views = take(sizeof(ViewParams) * V);
+    L.off_status = take(sizeof(FrameStatus) * V);
+    L.off_nt = take(4ull * V * N);
+    L.off_bounds = take(8ull * V * N);
+    L.off_rec = take(64ull * V * N);
+    L.off_bsums = take(4ull * V * nbp);
+    L.off_keys0 = take(static_cast<size_t>(key_bytes) * V * cap);
+    L.off_keys1 = take(static_cast<size_t>(key_bytes) * V * cap);
+    L.off_vals0 = take(4ull * V * cap);
+    L.off_vals1 = take(4ull * V * cap);
+    L.off_hist = take(4ull * V * kSortBins * sort_tiles);
+    L.off_dtot = take(4ull * V * kSortBins);
+    L.off_ranges = take(8ull * V * max_tiles);
+    L.off_map = take(4ull * V * max_tiles);
+    L.off_type = take(1ull * V * max_tiles);
+    L.off_ltype = take(1ull * V * max_large);
+    L.off_wf = take(4ull * V * max_large);
+    L.off_wl = take(4ull * V * max_large);
+    L.off_wm = take(4ull * V * max_large);
+    L.off_ctr = take(16);
+    for (int64_t f : temp_floats) L.temp_offsets.push_back(f > 0 ? take(4ull * f) : 0);
+    L.total = o;
+    return L;
+}
+
+fhtgs_status ensure_arena(fhtgs_context ctx, size_t bytes) {
+    if (bytes <= ctx->arena_bytes) return FHTGS_OK;
+    if (ctx->arena) {
+        FHTGS_CK(cudaDeviceSynchronize());
+        cudaFree(ctx->arena);
+        ctx->arena = nullptr;
+        ctx->arena_bytes = 0;
+    }
+    const size_t want = align_up(bytes + bytes / 8);
+    cudaError_t e = cudaMalloc(&ctx->arena, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ctx->arena = nullptr;
+        return fail(FHTGS_ERR_OUT_OF_MEMORY, "arena allocation of " + std::to_string(want) + " bytes failed: " +
+                                                 cudaGetErrorString(e));
+    }
+    ctx->arena_bytes = want;
+    return FHTGS_OK;
+}
+
+fhtgs_status validate(const fhtgs_primitives* p, const fhtgs_view* views, int n_views, const fhtgs_settings* s) {
+    if (!p || !views || !s) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
+    if (n_views <= 0) return fail(FHTGS_ERR_INVALID_ARGUMENT, "n_views must be positive");
+    if (p->n_primitives < 0) return fail(FHTGS_ERR_INVALID_ARGUMENT, "n_primitives must be >= 0");
+    if (p->total_sh_bases < 0) return fail(FHTGS_ERR_INVALID_ARGUMENT, "total_sh_bases must be >= 0");
+    if (p->n_primitives > 0 && (!p->positions || !p->scales || !p->rotations || !p->opacities || !p->sh_0))
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "null Gaussian attribute pointer");
+    if (s->active_sh_bases > 1 && s->active_sh_bases > p->total_sh_bases + 1)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "active_sh_bases exceeds 1 + sh_rest.size(1)");
+    if (s->active_sh_bases > 1 && p->n_primitives > 0 && !p->sh_rest)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "sh_rest is null but higher SH bands are active");
+    if (s->background_type < 0 || s->background_type > 3) return fail(FHTGS_ERR_INVALID_ARGUMENT, "unknown background model");
+    if (s->background_type != 0 && !s->background_data) return fail(FHTGS_ERR_INVALID_ARGUMENT, "background data is null");
+    if ((s->background_type == 2 || s->background_type == 3) && (s->texture_width <= 0 || s->texture_height <= 0))
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "texture background needs positive texture size");
+    for (int i = 0; i < n_views; ++i) {
+        const fhtgs_view& v = views[i];
+        if (v.width <= 0 || v.height <= 0) return fail(FHTGS_ERR_INVALID_ARGUMENT, "view size must be positive");
+        if (static_cast<int64_t>(v.width) * v.height > (1ll << 28))
+            return fail(FHTGS_ERR_INVALID_ARGUMENT, "view larger than 2^28 pixels");
+        const int64_t gl = (static_cast<int64_t>(v.width) + 15) / 16 * ((static_cast<int64_t>(v.height) + 15) / 16);
+        if (gl * kSubTiles + 1 >= (1ll << 31)) return fail(FHTGS_ERR_INVALID_ARGUMENT, "tile grid too large");
+        if ((v.width + 15) / 16 > 65535 || (v.height + 15) / 16 > 65535)
+            return fail(FHTGS_ERR_INVALID_ARGUMENT, "tile grid exceeds 16-bit bounds");
+        if (!v.M || !v.VPM || !v.VPR_inv || !v.cam_position || !v.visibility_mask || !v.visibility_mask_area_table ||
+            !v.fovea_mask_area_table || !v.image)
+            return fail(FHTGS_ERR_INVALID_ARGUMENT, "null view pointer");
+    }
+    return FHTGS_OK;
+}
+
+int64_t estimate_capacity(int64_t n_prims) {
+    int64_t c = std::max<int64_t>(int64_t(1) << 20, 12 * n_prims);
+    return (c + kSortTile - 1) / kSortTile * kSortTile;
+}
+
+fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views, int n_views,
+                         const fhtgs_settings* s, cudaStream_t stream) {
+    fhtgs_status st = validate(prims, views, n_views, s);
+    if (st != FHTGS_OK) return st;
+    FHTGS_CK(cudaSetDevice(ctx->device));
+    const int V = n_views;
+    const int64_t N = prims->n_primitives;
+    std::vector<ViewGeom> geo(V);
+    int max_tiles = 0, max_large = 0, end_bit = 0;
+    for (int i = 0; i < V; ++i) {
+        geo[i] = geometry(views[i]);
+        max_tiles = std::max(max_tiles, geo[i].n_tiles);
+        max_large = std::max(max_large, geo[i].n_large);
+        end_bit = std::max(end_bit, geo[i].end_bit);
+    }
+    if (ctx->cap <= 0) ctx->cap = estimate_capacity(N);
+    const int64_t cap = ctx->cap;
+    const int key_u32 = end_bit > 16 ? 1 : 0;
+    const int nbp = static_cast<int>((N + kPrimBlock - 1) / kPrimBlock);
+    const int sort_tiles = static_cast<int>((cap + kSortTile - 1) / kSortTile);
+    std::vector<int64_t> temp_floats(V, 0);
+    if (s->blur_periphery)
+        for (int i = 0; i < V; ++i) temp_floats[i] = 3ll * views[i].width * views[i].height;
+    Layout L = plan(V, N, nbp, cap, key_u32 ? 4 : 2, sort_tiles, max_tiles, max_large, temp_floats);
+    st = ensure_arena(ctx, L.total);
+    if (st != FHTGS_OK) return st;
+    char* A = ctx->arena;
+
+    FrameParams fp{};
+    fp.n_views = V;
+    fp.n_prims = static_cast<int>(N);
+    fp.total_sh = prims->total_sh_bases;
+    fp.active_sh = s->active_sh_bases;
+    fp.K = s->K;
+    fp.near_plane = s->near_plane;
+    fp.far_plane = s->far_plane;
+    fp.scale_modifier = s->scale_modifier;
+    fp.to_chw = s->to_chw ? 1 : 0;
+    fp.blur = s->blur_periphery ? 1 : 0;
+    fp.aaa = s->anti_aliasing ? 1 : 0;
+    fp.bg_type = s->background_type;
+    fp.bg_data = s->background_data;
+    fp.tex_w = s->texture_width;
+    fp.tex_h = s->texture_height;
+    fp.key_u32 = key_u32;
+    fp.end_bit = end_bit;
+    fp.cap = cap;
+    fp.max_tiles = max_tiles;
+    fp.max_large = max_large;
+    fp.n_blocks_prim = nbp;
+
+    FrameBuffers fb{};
+    fb.views = reinterpret_cast<ViewParams*>(A + L.off_views);
+    fb.status = reinterpret_cast<FrameStatus*>(A + L.off_status);
+    fb.n_touched = reinterpret_cast<uint32_t*>(A + L.off_nt);
+    fb.bounds = reinterpret_cast<ushort4*>(A + L.off_bounds);
+    fb.rec = reinterpret_cast<float4*>(A + L.off_rec);
+    fb.block_sums = reinterpret_cast<uint32_t*>(A + L.off_bsums);
+    fb.keys[0] = A + L.off_keys0;
+    fb.keys[1] = A + L.off_keys1;
+    fb.vals[0] = reinterpret_cast<uint32_t*>(A + L.off_vals0);
+    fb.vals[1] = reinterpret_cast<uint32_t*>(A + L.off_vals1);
+    fb.final_buf = 0;
+    fb.sort_hist = reinterpret_cast<uint32_t*>(A + L.off_hist);
+    fb.sort_digit_tot = reinterpret_cast<uint32_t*>(A + L.off_dtot);
+    fb.sort_tiles = N > 0 ? sort_tiles : 0;
+    fb.ranges = reinterpret_cast<uint2*>(A + L.off_ranges);
+    fb.tile_map_part = reinterpret_cast<uint32_t*>(A + L.off_map);
+    fb.tile_type_part = reinterpret_cast<uint8_t*>(A + L.off_type);
+    fb.large_type = reinterpret_cast<uint8_t*>(A + L.off_ltype);
+    fb.work_full = reinterpret_cast<uint32_t*>(A + L.off_wf);
+    fb.work_low = reinterpret_cast<uint32_t*>(A + L.off_wl);
+    fb.work_masked = reinterpret_cast<uint32_t*>(A + L.off_wm);
+    fb.counters = reinterpret_cast<uint32_t*>(A + L.off_ctr);
+
+    std::vector<ViewSetup> setups(V);
+    for (int i = 0; i < V; ++i) {
+        const fhtgs_view& v = views[i];
+        const ViewGeom& g = geo[i];
+        ViewSetup& su = setups[i];
+        su.M = v.M;
+        su.VPM = v.VPM;
+        su.VPR_inv = v.VPR_inv;
+        su.cam = v.cam_position;
+        ViewParams& p = su.p;
+        std::memset(&p, 0, sizeof(p));
+        p.gaze_px = make_float2(g.gaze_px, g.gaze_py);
+        p.gaze_tiles = make_float2(static_cast<float>(g.gaze_tx), static_cast<float>(g.gaze_ty));
+        p.gaze_tiles_i = make_int2(g.gaze_tx, g.gaze_ty);
+        p.width = v.width;
+        p.height = v.height;
+        p.focal_x = v.focal_x;
+        p.focal_y = v.focal_y;
+        p.center_x = v.center_x;
+        p.center_y = v.center_y;
+        p.glw = g.glw;
+        p.glh = g.glh;
+        p.n_large = g.n_large;
+        p.n_tiles = g.n_tiles;
+        p.vis_mask = v.visibility_mask;
+        p.vis_sat = v.visibility_mask_area_table;
+        p.fovea_sat = v.fovea_mask_area_table;
+        p.image = v.image;
+        p.work = s->blur_periphery ? reinterpret_cast<float*>(A + L.temp_offsets[i]) : v.image;
+    }
+    Gaussians gs{prims->positions, prims->scales, prims->rotations, prims->opacities, prims->sh_0, prims->sh_rest};
+    const KernelSet& ks = s->fast_math ? kernels_fast() : kernels_ieee();
+
+    const bool prof = ctx->profile;
+    cudaEvent_t* ev = ctx->ev[ctx->frames_profiled % kStageRing];
+    auto mark = [&](int i) {
+        if (prof) cudaEventRecord(ev[i], stream);
+    };
+    long long n = 0;
+    mark(0);
+    FHTGS_CK(cudaMemsetAsync(fb.counters, 0, 16, stream));
+    n += ks.setup(setups.data(), V, fb.views, stream);
+    n += ks.classify(fp, fb, stream);
+    mark(1);
+    n += ks.preprocess(fp, fb, gs, stream);
+    mark(2);
+    if (nbp > 0) {
+        n += ks.scan_blocks(fp, fb, stream);
+        n += ks.create_instances(fp, fb, stream);
+    }
+    mark(3);
+    n += ks.sort(fp, fb, stream);
+    mark(4);
+    n += ks.ranges(fp, fb, stream);
+    mark(5);
+    n += ks.blend(fp, fb, ctx->n_sms, stream, prof ? ev[6] : nullptr);
+    mark(7);
+    n += ks.compose(fp, fb, stream);
+    mark(8);
+    FHTGS_CK(cudaGetLastError());
+    ctx->launches += n;
+    if (prof) ++ctx->frames_profiled;
+
+    ctx->have_frame = true;
+    ctx->fp = fp;
+    ctx->fb = fb;
+    ctx->geo = geo;
+    ctx->views.assign(views, views + V);
+    ctx->stream = stream;
+    return FHTGS_OK;
+}
+
+fhtgs_status read_status(fhtgs_context ctx) {
+    const int V = ctx->fp.n_views;
+    if (ctx->h_status_n < V) {
+        if (ctx->h_status) cudaFreeHost(ctx->h_status);
+        ctx->h_status = nullptr;
+        FHTGS_CK(cudaMallocHost(&ctx->h_status, sizeof(FrameStatus) * V));
+        ctx->h_status_n = V;
+    }
+    FHTGS_CK(cudaMemcpyAsync(ctx->h_status, ctx->fb.status, sizeof(FrameStatus) * V, cudaMemcpyDeviceToHost, ctx->stream));
+    FHTGS_CK(cudaStreamSynchronize(ctx->stream));
+    return FHTGS_OK;
+}
+
+fhtgs_status render_sync_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views, int n_views,
+                              const fhtgs_settings* s, cudaStream_t stream) {
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        fhtgs_status st = render_impl(ctx, prims, views, n_views, s, stream);
+        if (st != FHTGS_OK) return st;
+        st = read_status(ctx);
+        if (st != FHTGS_OK) return st;
+        unsigned long long need = 0;
+        bool overflow = false;
+        for (int i = 0; i < n_views; ++i) {
+            need = std::max(need, ctx->h_status[i].n_instances);
+            overflow = overflow || ctx->h_status[i].n_instances > static_cast<unsigned long long>(ctx->cap);
+        }
+        if (!overflow) return FHTGS_OK;
+        int64_t grown = static_cast<int64_t>(need + need / 4 + kSortTile);
+        ctx->cap = (grown + kSortTile - 1) / kSortTile * kSortTile;
+    }
+    return fail(FHTGS_ERR_CAPACITY, "instance capacity still insufficient after regrowth");
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t fhtgs_abi_version(void) { return FHTGS_ABI_VERSION; }
+const char* fhtgs_last_error(void) { return g_error.c_str(); }
+
+fhtgs_status fhtgs_context_create(int32_t device, fhtgs_context* out) {
+    if (!out) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null output pointer");
+    *out = nullptr;
+    int n = 0;
+    FHTGS_CK(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) return fail(FHTGS_ERR_INVALID_ARGUMENT, "no such CUDA device");
+    FHTGS_CK(cudaSetDevice(device));
+    auto* c = new fhtgs_context_s();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->n_sms, cudaDevAttrMultiProcessorCount, device);
+    *out = c;
+    return FHTGS_OK;
+}
+
+fhtgs_status fhtgs_context_destroy(fhtgs_context ctx) {
+    if (!ctx) return FHTGS_OK;
+    cudaSetDevice(ctx->device);
+    for (auto& set : ctx->ev)
+        for (auto& e : set)
+            if (e) cudaEventDestroy(e);
+    if (ctx->arena) {
+        cudaDeviceSynchronize();
+        cudaFree(ctx->arena);
+    }
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    delete ctx;
+    return FHTGS_OK;
+}
+
+fhtgs_status fhtgs_context_reserve(fhtgs_context ctx, int32_t n_primitives, int32_t n_views, int32_t max_width,
+                                   int32_t max_height, int64_t instances_per_view) {
+    if (!ctx || n_primitives < 0 || n_views <= 0 || max_width <= 0 || max_height <= 0)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "invalid reserve request");
+    FHTGS_CK(cudaSetDevice(ctx->device));
+    int64_t cap = instances_per_view > 0 ? instances_per_view : estimate_capacity(n_primitives);
+    cap = (cap + kSortTile - 1) / kSortTile * kSortTile;
+    ctx->cap = std::max(ctx->cap, cap);
+    const int glw = (max_width + 15) / 16, glh = (max_height + 15) / 16;
+    const int n_large = glw * glh, n_tiles = 4 * n_large;
+    const int nbp = (n_primitives + kPrimBlock - 1) / kPrimBlock;
+    std::vector<int64_t> temp(n_views, 3ll * max_width * max_height);
+    Layout L = plan(n_views, n_primitives, nbp, ctx->cap, end_bit_of(n_tiles + 1) > 16 ? 4 : 2,
+                    static_cast<int>((ctx->cap + kSortTile - 1) / kSortTile), n_tiles, n_large, temp);
+    return ensure_arena(ctx, L.total);
+}
+
+size_t fhtgs_context_arena_bytes(fhtgs_context ctx) { return ctx ? ctx->arena_bytes : 0; }
+
+fhtgs_status fhtgs_context_set_profiling(fhtgs_context ctx, int32_t enable) {
+    if (!ctx) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null context");
+    FHTGS_CK(cudaSetDevice(ctx->device));
+    if (enable && !ctx->ev[0][0])
+        for (auto& set : ctx->ev)
+            for (auto& e : set) FHTGS_CK(cudaEventCreate(&e));
+    ctx->profile = enable != 0;
+    return FHTGS_OK;
+}
+
+fhtgs_status fhtgs_get_stage_times(fhtgs_context ctx, float* ms, int32_t n) {
+    if (!ctx || !ms || n < FHTGS_N_STAGES) return fail(FHTGS_ERR_INVALID_ARGUMENT, "need a buffer of FHTGS_N_STAGES floats");
+    if (!ctx->profile || ctx->frames_profiled == 0) return fail(FHTGS_ERR_NOT_READY, "profiling off or no frame rendered");
+    cudaEvent_t* ev = ctx->ev[(ctx->frames_profiled - 1) % kStageRing];
+    FHTGS_CK(cudaEventSynchronize(ev[kStageEvents - 1]));
+    for (int i = 0; i < FHTGS_N_STAGES; ++i) FHTGS_CK(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+    return FHTGS_OK;
+}
+
+fhtgs_status fhtgs_get_stage_history(fhtgs_context ctx, float* ms, int32_t max_frames, int32_t* n_frames) {
+    if (!ctx || !ms || !n_frames || max_frames <= 0) return fail(FHTGS_ERR_INVALID_ARGUMENT, "bad history request");
+    if (!ctx->profile || ctx->frames_profiled == 0) return fail(FHTGS_ERR_NOT_READY, "profiling off or no frame rendered");
+    const long long have = std::min<long long>(ctx->frames_profiled, kStageRing);
+    const int n = static_cast<int>(std::min<long long>(have, max_frames));
+    for (int f = 0; f < n; ++f) {
+        cudaEvent_t* ev = ctx->ev[(ctx->frames_profiled - n + f) % kStageRing];
+        FHTGS_CK(cudaEventSynchronize(ev[kStageEvents - 1]));
+        for (int i = 0; i < FHTGS_N_STAGES; ++i)
+            FHTGS_CK(cudaEventElapsedTime(&ms[f * FHTGS_N_STAGES + i], ev[i], ev[i + 1]));
+    }
+    *n_frames = n;
+    return FHTGS_OK;
+}
+
+int64_t fhtgs_context_launch_count(fhtgs_context ctx) { return ctx ? ctx->launches : 0; }
+
+fhtgs_status fhtgs_render_views(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views,
+                                int32_t n_views, const fhtgs_settings* settings, void* stream) {
+    if (!ctx) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null context");
+    return render_impl(ctx, prims, views, n_views, settings, static_cast<cudaStream_t>(stream));
+}
+
+fhtgs_status fhtgs_render_views_sync(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views,
+                                     int32_t n_views, const fhtgs_settings* settings, void* stream) {
+    if (!ctx) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null context");
+    return render_sync_impl(ctx, prims, views, n_views, settings, static_cast<cudaStream_t>(stream));
+}
+
+fhtgs_status fhtgs_get_frame_info(fhtgs_context ctx, int32_t view, fhtgs_frame_info* out) {
+    if (!ctx || !out) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
+    if (!ctx->have_frame) return fail(FHTGS_ERR_NOT_READY, "no frame rendered yet");
+    if (view < 0 || view >= ctx->fp.n_views) return fail(FHTGS_ERR_INVALID_ARGUMENT, "view index out of range");
+    fhtgs_status st = read_status(ctx);
+    if (st != FHTGS_OK) return st;
+    const FrameStatus& s = ctx->h_status[view];
+    out->n_instances = static_cast<int64_t>(s.n_instances);
+    out->instance_capacity = ctx->fp.cap;
+    out->n_active_tiles = s.n_active;
+    for (int k = 0; k < 6; ++k) out->partition_ranges[k] = s.ranges[k];
+    out->overflow = s.n_instances > static_cast<unsigned long long>(ctx->fp.cap) ? 1 : 0;
+    out->end_bit = ctx->fp.end_bit;
+    return FHTGS_OK;
+}
+
+fhtgs_status fhtgs_copy_intermediates(fhtgs_context ctx, int32_t view, fhtgs_intermediates* out) {
+    if (!ctx || !out) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
+    if (!ctx->have_frame) return fail(FHTGS_ERR_NOT_READY, "no frame rendered yet");
+    if (view < 0 || view >= ctx->fp.n_views) return fail(FHTGS_ERR_INVALID_ARGUMENT, "view index out of range");
+    fhtgs_status st = read_status(ctx);
+    if (st != FHTGS_OK) return st;
+    const FrameParams& fp = ctx->fp;
+    const FrameBuffers& fb = ctx->fb;
+    const FrameStatus& s = ctx->h_status[view];
+    const size_t N = static_cast<size_t>(fp.n_prims);
+    const size_t vo = static_cast<size_t>(view) * N;
+    if (out->n_touched && N) FHTGS_CK(cudaMemcpy(out->n_touched, fb.n_touched + vo, 4 * N, cudaMemcpyDeviceToHost));
+    if (out->screen_bounds && N) FHTGS_CK(cudaMemcpy(out->screen_bounds, fb.bounds + vo, 8 * N, cudaMemcpyDeviceToHost));
+    if ((out->vpmt || out->rgba) && N) {
+        std::vector<float4> rec(4 * N);
+        FHTGS_CK(cudaMemcpy(rec.data(), fb.rec + 4 * vo, 64 * N, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < N; ++i) {
+            if (out->vpmt) std::memcpy(out->vpmt + 12 * i, &rec[4 * i], 48);
+            if (out->rgba) std::memcpy(out->rgba + 4 * i, &rec[4 * i + 3], 16);
+        }
+    }
+    const size_t T = static_cast<size_t>(ctx->geo[view].n_tiles);
+    const size_t na = s.n_active;
+    if (out->tile_index_map_partitioned && na)
+        FHTGS_CK(cudaMemcpy(out->tile_index_map_partitioned, fb.tile_map_part + static_cast<size_t>(view) * fp.max_tiles,
+                            4 * na, cudaMemcpyDeviceToHost));
+    if (out->tile_type_partitioned && na)
+        FHTGS_CK(cudaMemcpy(out->tile_type_partitioned, fb.tile_type_part + static_cast<size_t>(view) * fp.max_tiles, na,
+                            cudaMemcpyDeviceToHost));
+    const size_t M = static_cast<size_t>(std::min<unsigned long long>(s.n_instances, static_cast<unsigned long long>(fp.cap)));
+    if (out->keys && M) {
+        if (fp.key_u32) {
+            FHTGS_CK(cudaMemcpy(out->keys, static_cast<uint32_t*>(fb.keys[fb.final_buf]) + static_cast<size_t>(view) * fp.cap,
+                                4 * M, cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<uint16_t> k(M);
+            FHTGS_CK(cudaMemcpy(k.data(), static_cast<uint16_t*>(fb.keys[fb.final_buf]) + static_cast<size_t>(view) * fp.cap,
+                                2 * M, cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < M; ++i) out->keys[i] = k[i];
+        }
+    }
+    if (out->values && M)
+        FHTGS_CK(cudaMemcpy(out->values, fb.vals[fb.final_buf] + static_cast<size_t>(view) * fp.cap, 4 * M,
+                            cudaMemcpyDeviceToHost));
+    if (out->instance_ranges && T)
+        FHTGS_CK(cudaMemcpy(out->instance_ranges, fb.ranges + static_cast<size_t>(view) * fp.max_tiles, 8 * T,
+                            cudaMemcpyDeviceToHost));
+    return FHTGS_OK;
+}
+
+static fhtgs_status mono_common(fhtgs_context ctx, int fast, const float* positions, const float* scales,
+                                const float* rotations, const float* opacities, const float* sh_0, const float* sh_rest,
+                                int32_t n_primitives, int32_t total_sh_bases, const float* M, const float* VPM,
+                                const float* VPR_inv, const float* cam_position, float gaze_x, float gaze_y,
+                                const uint32_t* visibility_mask, const uint32_t* visibility_mask_area_table,
+                                const uint32_t* fovea_mask_area_table, const float* background_model_data,
+                                int32_t texture_width, int32_t texture_height, int32_t background_model_type, int32_t K,
+                                int32_t active_sh_bases, int32_t width, int32_t height, float focal_x, float focal_y,
+                                float center_x, float center_y, float near_plane, float far_plane, float scale_modifier,
+                                int32_t to_chw, int32_t blur_periphery, int32_t anti_aliasing, float* image,
+                                void* stream) {
+    if (!ctx) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null context");
+    fhtgs_primitives p{positions, scales, rotations, opacities, sh_0, sh_rest, n_primitives, total_sh_bases};
+    fhtgs_view v{};
+    v.M = M; v.VPM = VPM; v.VPR_inv = VPR_inv; v.cam_position = cam_position;
+    v.gaze_x = gaze_x; v.gaze_y = gaze_y;
+    v.visibility_mask = visibility_mask; v.visibility_mask_area_table = visibility_mask_area_table;
+    v.fovea_mask_area_table = fovea_mask_area_table;
+    v.width = width; v.height = height; v.focal_x = focal_x; v.focal_y = focal_y; v.center_x = center_x; v.center_y = center_y;
+    v.image = image;
+    fhtgs_settings s{};
+    s.K = K; s.active_sh_bases = active_sh_bases; s.near_plane = near_plane; s.far_plane = far_plane;
+    s.scale_modifier = scale_modifier; s.to_chw = to_chw; s.blur_periphery = blur_periphery; s.anti_aliasing = anti_aliasing;
+    s.background_type = background_model_type; s.background_data = background_model_data;
+    s.texture_width = texture_width; s.texture_height = texture_height; s.fast_math = fast;
+    return render_sync_impl(ctx, &p, &v, 1, &s, static_cast<cudaStream_t>(stream));
+}
+
+fhtgs_status fhtgs_render_mono(fhtgs_context ctx, const float* positions, const float* scales, const float* rotations,
+                               const float* opacities, const float* sh_0, const float* sh_rest, int32_t n_primitives,
+                               int32_t total_sh_bases, const float* M, const float* VPM, const float* VPR_inv,
+                               const float* cam_position, float gaze_x, float gaze_y, const uint32_t* visibility_mask,
+                               const uint32_t* visibility_mask_area_table, const uint32_t* fovea_mask_area_table,
+                               const float* background_model_data, int32_t texture_width, int32_t texture_height,
+                               int32_t background_model_type, int32_t K, int32_t active_sh_bases, int32_t width,
+                               int32_t height, float focal_x, float focal_y, float center_x, float center_y,
+                               float near_plane, float far_plane, float scale_modifier, int32_t to_chw,
+                               int32_t blur_periphery, int32_t anti_aliasing, float* image, void* stream) {
+    return mono_common(ctx, 0, positions, scales, rotations, opacities, sh_0, sh_rest, n_primitives, total_sh_bases, M,
+                       VPM, VPR_inv, cam_position, gaze_x, gaze_y, visibility_mask, visibility_mask_area_table,
+                       fovea_mask_area_table, background_model_data, texture_width, texture_height,
+                       background_model_type, K, active_sh_bases, width, height, focal_x, focal_y, center_x, center_y,
+                       near_plane, far_plane, scale_modifier, to_chw, blur_periphery, anti_aliasing, image, stream);
+}
+
+fhtgs_status fhtgs_benchmark_mono(fhtgs_context ctx, const float* positions, const float* scales, const float* rotations,
+                                  const float* opacities, const float* sh_0, const float* sh_rest, int32_t n_primitives,
+                                  int32_t total_sh_bases, const float* M, const float* VPM, const float* VPR_inv,
+                                  const float* cam_position, float gaze_x, float gaze_y, const uint32_t* visibility_mask,
+                                  const uint32_t* visibility_mask_area_table, const uint32_t* fovea_mask_area_table,
+                                  const float* background_model_data, int32_t texture_width, int32_t texture_height,
+                                  int32_t background_model_type, int32_t K, int32_t active_sh_bases, int32_t width,
+                                  int32_t height, float focal_x, float focal_y, float center_x, float center_y,
+                                  float near_plane, float far_plane, float scale_modifier, int32_t to_chw,
+                                  int32_t blur_periphery, int32_t anti_aliasing, float* image, void* stream) {
+    return mono_common(ctx, 1, positions, scales, rotations, opacities, sh_0, sh_rest, n_primitives, total_sh_bases, M,
+                       VPM, VPR_inv, cam_position, gaze_x, gaze_y, visibility_mask, visibility_mask_area_table,
+                       fovea_mask_area_table, background_model_data, texture_width, texture_height,
+                       background_model_type, K, active_sh_bases, width, height, focal_x, focal_y, center_x, center_y,
+                       near_plane, far_plane, scale_modifier, to_chw, blur_periphery, anti_aliasing, image, stream);
+}
+
+fhtgs_status fhtgs_render_stereo(
+    fhtgs_context ctx, const float* positions, const float* scales, const float* rotations, const float* opacities,
+    const float* sh_0, const float* sh_rest, int32_t n_primitives, int32_t total_sh_bases, const float* M_left,
+    const float* VPM_left, const float* VPR_inv_left, const float* cam_position_left, float gaze_x_left,
+    float gaze_y_left, const uint32_t* visibility_mask_left, const uint32_t* visibility_mask_area_table_left,
+    const uint32_t* fovea_mask_area_table_left, const float* background_model_data_left, int32_t texture_width_left,
+    int32_t texture_height_left, int32_t background_model_type_left, int32_t K_left, int32_t active_sh_bases_left,
+    int32_t width_left, int32_t height_left, float focal_x_left, float focal_y_left, float center_x_left,
+    float center_y_left, float near_plane_left, float far_plane_left, float scale_modifier_left, const float* M_right,
+    const float* VPM_right, const float* VPR_inv_right, const float* cam_position_right, float gaze_x_right,
+    float gaze_y_right, const uint32_t* visibility_mask_right, const uint32_t* visibility_mask_area_table_right,
+    const uint32_t* fovea_mask_area_table_right, int32_t width_right, int32_t height_right, float focal_x_right,
+    float focal_y_right, float center_x_right, float center_y_right, int32_t to_chw, int32_t blur_periphery,
+    int32_t anti_aliasing, float* image_left, float* image_right, void* stream) {
+    if (!ctx) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null context");
+    fhtgs_primitives p{positions, scales, rotations, opacities, sh_0, sh_rest, n_primitives, total_sh_bases};
+    fhtgs_view v[2] = {};
+    v[0].M = M_left; v[0].VPM = VPM_left; v[0].VPR_inv = VPR_inv_left; v[0].cam_position = cam_position_left;
+    v[0].gaze_x = gaze_x_left; v[0].gaze_y = gaze_y_left;
+    v[0].visibility_mask = visibility_mask_left; v[0].visibility_mask_area_table = visibility_mask_area_table_left;
+    v[0].fovea_mask_area_table = fovea_mask_area_table_left;
+    v[0].width = width_left; v[0].height = height_left; v[0].focal_x = focal_x_left; v[0].focal_y = focal_y_left;
+    v[0].center_x = center_x_left; v[0].center_y = center_y_left; v[0].image = image_left;
+    v[1].M = M_right; v[1].VPM = VPM_right; v[1].VPR_inv = VPR_inv_right; v[1].cam_position = cam_position_right;
+    v[1].gaze_x = gaze_x_right; v[1].gaze_y = gaze_y_right;
+    v[1].visibility_mask = visibility_mask_right; v[1].visibility_mask_area_table = visibility_mask_area_table_right;
+    v[1].fovea_mask_area_table = fovea_mask_area_table_right;
+    v[1].width = width_right; v[1].height = height_right; v[1].focal_x = focal_x_right; v[1].focal_y = focal_y_right;
+    v[1].center_x = center_x_right; v[1].center_y = center_y_right; v[1].image = image_right;
+    fhtgs_settings s{};
+    s.K = K_left; s.active_sh_bases = active_sh_bases_left; s.near_plane = near_plane_left; s.far_plane = far_plane_left;
+    s.scale_modifier = scale_modifier_left; s.to_chw = to_chw; s.blur_periphery = blur_periphery;
+    s.anti_aliasing = anti_aliasing; s.background_type = background_model_type_left;
+    s.background_data = background_model_data_left; s.texture_width = texture_width_left;
+    s.texture_height = texture_height_left; s.fast_math = 1;
+    return render_sync_impl(ctx, &p, v, 2, &s, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,1302 @@
+// fhtgs device kernels.  Included by kernels_fast.cu (-use_fast_math, the arithmetic of the
+// reference's _C_benchmarking / _C_stereo modules) and kernels_ieee.cu (the arithmetic of the
+// reference's _C module) with FHTGS_FLAVOR naming the namespace.
+//
+// Pipeline of one frame, all views of the frame in the same launches, no host round trip:
+//   setup      gather per-view camera matrices into ViewParams
+//   classify   large-tile classification + compaction (one block per view)
+//   preprocess one thread per Gaussian for all views: cull, project, bounds, SH colour
+//   scan       exclusive scan of the preprocess blocks' touched-tile sums -> M per view
+//   create     tile|sub-tile keys + primitive values, sentinel fill of over-counted slots
+//   sort       stable LSD radix sort of (key, value) pairs, 8-bit digits
+//   ranges     [begin, end) per small tile from key boundaries
+//   blend      K-buffer blend; full-res 16x16 tiles (fovea, blended) and 2x-down 16x16
+//              tiles (periphery), persistent blocks pulling tiles from a work counter
+//   compose    periphery bilinear upsampling / blur and blended-ring cross-fade
+#pragma once
+#include "fhtgs_math.cuh"
+#include "fhtgs_types.cuh"
+
+#ifndef FHTGS_FLAVOR
+#error "FHTGS_FLAVOR must name the math flavour namespace"
+#endif
+
+namespace fhtgs {
+namespace FHTGS_FLAVOR {
+using namespace fhtgs::vm;
+
+// ------------------------------------------------------------------------------------------
+// helpers
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T x) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// Block-wide exclusive scan (blockDim.x multiple of 32, <= 1024).  `total` receives the sum.
+template <typename T>
+__device__ __forceinline__ T block_excl_scan(T x, T& total, T* s_warp /* >= 32 entries */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    T incl = warp_incl_scan(x);
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < nw ? s_warp[lane] : T(0);
+        T wi = warp_incl_scan(w);
+        if (lane < nw) s_warp[lane] = wi - w;
+        if (lane == nw - 1) s_warp[32] = wi;
+    }
+    __syncthreads();
+    T res = incl - x + s_warp[warp];
+    total = s_warp[32];
+    __syncthreads();
+    return res;
+}
+
+__device__ __forceinline__ bool tile_visible(const uint32_t* mask, uint32_t tile) {
+    return (mask[tile / 32u] & (1u << (tile % 32u))) != 0;
+}
+
+// Tile-centre-in-circle test of the foveation (shared_kernels.cuh:155-220 and
+// kernel_utils.cuh:43-73 of the reference use the same float arithmetic).
+template <int radius>
+__device__ __forceinline__ bool in_fovea(uint32_t tx, uint32_t ty, float2 gaze_tiles) {
+    constexpr float r2 = static_cast<float>(radius * radius);
+    const float2 d = make_float2(__uint2float_rn(tx) + 0.5f, __uint2float_rn(ty) + 0.5f) - gaze_tiles;
+    return dot(d, d) < r2;
+}
+
+__device__ __forceinline__ float4 ld4(const float* p) { return make_float4(p[0], p[1], p[2], p[3]); }
+
+// ------------------------------------------------------------------------------------------
+// setup
+// ------------------------------------------------------------------------------------------
+constexpr int kSetupChunk = 8;
+struct SetupChunk {
+    ViewSetup v[kSetupChunk];
+    int n, first;
+};
+
+__global__ void setup_kernel(SetupChunk c, ViewParams* __restrict__ out) {
+    const int i = threadIdx.x;
+    if (i >= c.n) return;
+    ViewParams p = c.v[i].p;
+    for (int r = 0; r < 3; ++r) p.M[r] = ld4(c.v[i].M + 4 * r);
+    for (int r = 0; r < 4; ++r) p.VPM[r] = ld4(c.v[i].VPM + 4 * r);
+    for (int r = 0; r < 4; ++r) p.VPR_inv[r] = ld4(c.v[i].VPR_inv + 4 * r);
+    p.cam = make_float4(c.v[i].cam[0], c.v[i].cam[1], c.v[i].cam[2], 0.0f);
+    out[c.first + i] = p;
+}
+
+int launch_setup(const ViewSetup* setups, int n_views, ViewParams* out, cudaStream_t s) {
+    int n = 0;
+    for (int first = 0; first < n_views; first += kSetupChunk) {
+        SetupChunk c;
+        c.n = n_views - first < kSetupChunk ? n_views - first : kSetupChunk;
+        c.first = first;
+        for (int i = 0; i < c.n; ++i) c.v[i] = setups[first + i];
+        setup_kernel<<<1, 32, 0, s>>>(c, out);
+        ++n;
+    }
+    return n;
+}
+
+// ------------------------------------------------------------------------------------------
+// tile classification + compaction (replaces fill_tile_index_num_tiles, the scan,
+// build_tile_index_map, the 2-bit type sort and get_partition_ranges_cu of the reference,
+// shared_kernels.cuh:155-238, inference.cu:131-188, with one block per view)
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint8_t large_tile_type(const ViewParams& vp, uint32_t tile) {
+    if (!tile_visible(vp.vis_mask, tile)) return kMasked;
+    const uint32_t tx = tile % static_cast<uint32_t>(vp.glw), ty = tile / static_cast<uint32_t>(vp.glw);
+    if (in_fovea<kFoveaRadiusTiles>(tx, ty, vp.gaze_tiles))
+        return in_fovea<kBlendRadiusTiles>(tx, ty, vp.gaze_tiles) ? kFovea : kBlended;
+    return kPeriphery;
+}
+
+__global__ void __launch_bounds__(1024) classify_kernel(FrameParams fp, FrameBuffers fb) {
+    __shared__ unsigned long long s_warp[33];
+    const int v = blockIdx.x;
+    const ViewParams& vp = fb.views[v];
+    const int TL = vp.n_large;
+    const int seg = (TL + blockDim.x - 1) / blockDim.x;
+    const int b0 = min(TL, static_cast<int>(threadIdx.x) * seg), b1 = min(TL, b0 + seg);
+    uint32_t cnt[4] = {0, 0, 0, 0};
+    for (int t = b0; t < b1; ++t) cnt[large_tile_type(vp, t)]++;
+    // two packed 64-bit scans: (fovea | periphery << 32), (blended | masked << 32)
+    unsigned long long tot0, tot1;
+    unsigned long long e0 = block_excl_scan<unsigned long long>(cnt[0] | (static_cast<unsigned long long>(cnt[1]) << 32), tot0, s_warp);
+    unsigned long long e1 = block_excl_scan<unsigned long long>(cnt[2] | (static_cast<unsigned long long>(cnt[3]) << 32), tot1, s_warp);
+    const uint32_t nF = static_cast<uint32_t>(tot0), nP = static_cast<uint32_t>(tot0 >> 32);
+    const uint32_t nB = static_cast<uint32_t>(tot1), nM = static_cast<uint32_t>(tot1 >> 32);
+    uint32_t oF = static_cast<uint32_t>(e0), oP = static_cast<uint32_t>(e0 >> 32);
+    uint32_t oB = static_cast<uint32_t>(e1), oM = static_cast<uint32_t>(e1 >> 32);
+    const uint32_t n_active = kSubTiles * nF + nP + kSubTiles * nB;
+    // The reference renders nothing when exactly one small-tile entry is active (its
+    // partition-range kernel starts at index 1, shared_kernels.cuh:222-238); that tile is then
+    // cleared instead of blended, which matches the zero-initialised output of _C.
+    const bool none = n_active <= 1;
+    uint32_t* map = fb.tile_map_part + static_cast<size_t>(v) * fp.max_tiles;
+    uint8_t* typ = fb.tile_type_part + static_cast<size_t>(v) * fp.max_tiles;
+    uint8_t* lt = fb.large_type + static_cast<size_t>(v) * fp.max_large;
+    uint32_t* wf = fb.work_full + static_cast<size_t>(v) * fp.max_large;
+    uint32_t* wl = fb.work_low + static_cast<size_t>(v) * fp.max_large;
+    uint32_t* wm = fb.work_masked + static_cast<size_t>(v) * fp.max_large;
+    for (int t = b0; t < b1; ++t) {
+        const uint8_t ty = large_tile_type(vp, t);
+        lt[t] = ty;
+        const uint32_t sub0 = static_cast<uint32_t>(t) * kSubTiles;
+        if (ty == kFovea) {
+            for (int i = 0; i < kSubTiles; ++i) { map[kSubTiles * oF + i] = sub0 + i; typ[kSubTiles * oF + i] = kFovea; }
+            wf[oF++] = t;
+        } else if (ty == kPeriphery) {
+            map[kSubTiles * nF + oP] = sub0; typ[kSubTiles * nF + oP] = kPeriphery;
+            if (none) wm[nM] = t; else wl[oP] = t;
+            ++oP;
+        } else if (ty == kBlended) {
+            const uint32_t base = kSubTiles * nF + nP + kSubTiles * oB;
+            for (int i = 0; i < kSubTiles; ++i) { map[base + i] = sub0 + i; typ[base + i] = kBlended; }
+            wf[nF + oB++] = t;
+        } else {
+            wm[oM++] = t;
+        }
+    }
+    if (threadIdx.x == 0) {
+        FrameStatus& st = fb.status[v];
+        st.n_active = n_active;
+        for (int k = 0; k < 6; ++k) st.ranges[k] = 0;
+        if (!none) {
+            if (nF) { st.ranges[0] = 0; st.ranges[1] = kSubTiles * nF; }
+            if (nP) { st.ranges[2] = kSubTiles * nF; st.ranges[3] = kSubTiles * nF + nP; }
+            if (nB) { st.ranges[4] = kSubTiles * nF + nP; st.ranges[5] = n_active; }
+        }
+        st.n_fovea_large = nF;
+        st.n_blended_large = nB;
+        st.n_periphery_large = none ? 0 : nP;
+        st.n_masked_large = none ? nM + nP : nM;
+        st.overflow = 0;
+        st.n_instances = 0;
+    }
+}
+
+int launch_classify(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s) {
+    classify_kernel<<<fp.n_views, 1024, 0, s>>>(fp, fb);
+    return 1;
+}
+
+// ------------------------------------------------------------------------------------------
+// preprocess (restates preprocess_cu / transform_and_cull / convert_sh_to_color of the
+// reference, inference.cuh:42-136, kernel_utils.cuh:76-213, sh_utils.cuh:8-69, with the same
+// expression structure; one thread per Gaussian, all views per thread)
+// ------------------------------------------------------------------------------------------
+struct Mat3 { float r11, r12, r13, r21, r22, r23, r31, r32, r33; };
+
+__device__ __forceinline__ Mat3 quat_to_rot(const float4 q) {
+    const float r = q.x, x = q.y, y = q.z, z = q.w;
+    const float xx = x * x, yy = y * y, zz = z * z;
+    const float xy = x * y, xz = x * z, yz = y * z;
+    const float rx = r * x, ry = r * y, rz = r * z;
+    return {1.0f - 2.0f * (yy + zz), 2.0f * (xy - rz), 2.0f * (xz + ry),
+            2.0f * (xy + rz), 1.0f - 2.0f * (xx + zz), 2.0f * (yz - rx),
+            2.0f * (xz - ry), 2.0f * (yz + rx), 1.0f - 2.0f * (xx + yy)};
+}
+
+// Real spherical-harmonics basis constants (degree <= 3).
+constexpr float kC0 = 0.28209479177387814f, kC1 = 0.48860251190291987f;
+constexpr float kC2a = 1.0925484305920792f, kC2b = 0.94617469575755997f, kC2c = 0.31539156525251999f,
+                kC2d = 0.54627421529603959f;
+constexpr float kC3a = 0.59004358992664352f, kC3b = 1.7701307697799304f, kC3c = 2.8906114426405538f,
+                kC3d = 0.45704579946446572f, kC3e = 2.2852289973223288f, kC3f = 1.865881662950577f,
+                kC3g = 1.1195289977703462f, kC3h = 1.4453057213202769f;
+
+__device__ __forceinline__ float3 sh_to_rgb(const float* __restrict__ sh0, const float* __restrict__ rest,
+                                            float3 pos, float3 cam, int active) {
+    float3 res = 0.5f + kC0 * ld3(sh0);
+    if (active > 1) {
+        const float3 d = normalize(pos - cam);
+        const float x = d.x, y = d.y, z = d.z;
+        res = res - kC1 * y * ld3(rest + 0) + kC1 * z * ld3(rest + 3) - kC1 * x * ld3(rest + 6);
+        if (active > 4) {
+            const float xx = x * x, yy = y * y, zz = z * z;
+            const float xy = x * y, xz = x * z, yz = y * z;
+            res = res + kC2a * xy * ld3(rest + 9) - kC2a * yz * ld3(rest + 12) + (kC2b * zz - kC2c) * ld3(rest + 15)
+                      - kC2a * xz * ld3(rest + 18) + kC2d * (xx - yy) * ld3(rest + 21);
+            if (active > 9) {
+                res = res + y * (kC3a * yy - kC3b * xx) * ld3(rest + 24) + kC3c * xy * z * ld3(rest + 27)
+                          + y * (kC3d - kC3e * zz) * ld3(rest + 30) + z * (kC3f * zz - kC3g) * ld3(rest + 33)
+                          + x * (kC3d - kC3e * zz) * ld3(rest + 36) + kC3h * z * (xx - yy) * ld3(rest + 39)
+                          + x * (kC3b * yy - kC3a * xx) * ld3(rest + 42);
+            }
+        }
+    }
+    return res;
+}
+
+__device__ __forceinline__ uint32_t touched_from_bounds(const ViewParams& vp, const uint4 b) {
+    const int diam = 2 * kFoveaRadiusTiles;
+    const int tlx = vp.gaze_tiles_i.x - kFoveaRadiusTiles, tly = vp.gaze_tiles_i.y - kFoveaRadiusTiles;
+    const uint4 fb = make_uint4(min(diam, max(0, static_cast<int>(b.x) - tlx)), min(diam, max(0, static_cast<int>(b.y) - tlx)),
+                                min(diam, max(0, static_cast<int>(b.z) - tly)), min(diam, max(0, static_cast<int>(b.w) - tly)));
+    const uint32_t W1 = static_cast<uint32_t>(vp.glw) + 1u;
+    const uint32_t* sat = vp.vis_sat;
+    uint32_t n = sat[b.y + W1 * b.w] + sat[b.x + W1 * b.z] - sat[b.y + W1 * b.z] - sat[b.x + W1 * b.w];
+    if (fb.y != fb.x && fb.w != fb.z) {
+        const uint32_t F1 = static_cast<uint32_t>(diam) + 1u;
+        const uint32_t* f = vp.fovea_sat;
+        n += f[fb.y + F1 * fb.w] + f[fb.x + F1 * fb.z] - f[fb.y + F1 * fb.z] - f[fb.x + F1 * fb.w];
+    }
+    return n;
+}
+
+__device__ __forceinline__ float4 xform_row(const float4 P, float3 u, float3 v, float3 w, float3 pos) {
+    const float3 n = xyz(P);
+    return make_float4(dot(n, u), dot(n, v), dot(n, w), dot(n, pos) + P.w);
+}
+
+// Standard (non anti-aliased) transform and cull.  Returns true when culled.
+__device__ __forceinline__ bool transform_and_cull(const ViewParams& vp, const FrameParams& fp, float3 pos,
+                                                   float3 scale, float4 quat, float opacity, float4& P1,
+                                                   float4& P2, float4& P4, uint4& b, uint32_t& n) {
+    const float4 M3 = vp.M[2];
+    const float z = dot(xyz(M3), pos) + M3.w;
+    if (z < fp.near_plane || z > fp.far_plane) return true;
+    const Mat3 R = quat_to_rot(quat);
+    const float3 u = make_float3(R.r11 * scale.x, R.r21 * scale.x, R.r31 * scale.x) * fp.scale_modifier;
+    const float3 v = make_float3(R.r12 * scale.y, R.r22 * scale.y, R.r32 * scale.y) * fp.scale_modifier;
+    const float3 w = make_float3(R.r13 * scale.z, R.r23 * scale.z, R.r33 * scale.z) * fp.scale_modifier;
+    P4 = xform_row(vp.VPM[3], u, v, w, pos);
+    const float rho_cutoff = 2.0f * logf(opacity * kMinAlphaRcp);
+    const float4 d = make_float4(rho_cutoff, rho_cutoff, rho_cutoff, -1.0f);
+    const float s = dot(d, P4 * P4);
+    if (s == 0.0f) return true;
+    const float4 f = (1.0f / s) * d;
+    const float4 P3 = xform_row(vp.VPM[2], u, v, w, pos);
+    const float cz = dot(f, P3 * P4);
+    const float ez = sqrtf(fmaxf(cz * cz - dot(f, P3 * P3), 0.0f));
+    if (cz - ez < -1.0f || cz + ez > 1.0f) return true;
+    P1 = xform_row(vp.VPM[0], u, v, w, pos);
+    const float cx = dot(f, P1 * P4);
+    const float ex = sqrtf(fmaxf(cx * cx - dot(f, P1 * P1), 0.0f));
+    P2 = xform_row(vp.VPM[1], u, v, w, pos);
+    const float cy = dot(f, P2 * P4);
+    const float ey = sqrtf(fmaxf(cy * cy - dot(f, P2 * P2), 0.0f));
+    const uint32_t gw = static_cast<uint32_t>(vp.glw), gh = static_cast<uint32_t>(vp.glh);
+    const float tw = static_cast<float>(kTileLarge);
+    b = make_uint4(min(gw, static_cast<uint32_t>(max(0, __float2int_rd((cx - ex + 0.5f) / tw)))),
+                   min(gw, static_cast<uint32_t>(max(0, __float2int_ru((cx + ex + 0.5f) / tw)))),
+                   min(gh, static_cast<uint32_t>(max(0, __float2int_rd((cy - ey + 0.5f) / tw)))),
+                   min(gh, static_cast<uint32_t>(max(0, __float2int_ru((cy + ey + 0.5f) / tw)))));
+    n = touched_from_bounds(vp, b);
+    return n == 0;
+}
+
+// ---- anti-aliased variant (restates kernel_utils_aaa.cuh:9-363) ----
+__device__ __forceinline__ float max_contrib_plane(float4 plane, float4 P1, float4 P2, float4 P3, float4 P4, float4& out) {
+    const float norm = plane.w / (plane.x * plane.x + plane.y * plane.y + plane.z * plane.z);
+    const float4 mp = -norm * plane;
+    out.x = dot(xyz(P1), xyz(mp)) + P1.w;
+    out.y = dot(xyz(P2), xyz(mp)) + P2.w;
+    out.z = dot(xyz(P3), xyz(mp)) + P3.w;
+    out.w = dot(xyz(P4), xyz(mp)) + P4.w;
+    return -mp.w;
+}
+__device__ __forceinline__ float max_contrib_ray(float4 a, float4 b, float4 P1, float4 P2, float4 P3, float4 P4, float4& out) {
+    const float3 d = make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+    const float3 m = make_float3(a.w * b.x - a.x * b.w, a.w * b.y - a.y * b.w, a.w * b.z - a.z * b.w);
+    const float dd = dot(d, d);
+    const float3 mdd = make_float3(m.x / dd, m.y / dd, m.z / dd);
+    const float3 mp = cross(d, mdd);
+    out.x = dot(xyz(P1), mp) + P1.w;
+    out.y = dot(xyz(P2), mp) + P2.w;
+    out.z = dot(xyz(P3), mp) + P3.w;
+    out.w = dot(xyz(P4), mp) + P4.w;
+    return dot(m, mdd);
+}
+__device__ __forceinline__ bool in_screen_range(float p, float from, float ext, float ph) {
+    const float d = p - from * ph;
+    return d > 0.0f && d < ext * ph;
+}
+__device__ float max_contrib_frustum(float4 P1, float4 P2, float4 P3, float4 P4, float width, float height) {
+    float best = 3.402823466e+38f;
+    const float3 from = make_float3(0.0f, 0.0f, -1.0f);
+    const float3 ext = make_float3(width - 1.0f, height - 1.0f, 2.0f);
+    const float3 d = make_float3(P1.w - from.x * P4.w, P2.w - from.y * P4.w, P3.w - from.z * P4.w);
+    const bool bx = d.x > 0.0f && d.x < ext.x * P4.w;
+    const bool by = d.y > 0.0f && d.y < ext.y * P4.w;
+    const bool bz = d.z > 0.0f && d.z < ext.z * P4.w;
+    if (bx && by && bz) return 0.0f;
+    const float dx = copysignf(ext.x * 0.5f, d.x - (ext.x * 0.5f * P4.w));
+    const float dy = copysignf(ext.y * 0.5f, d.y - (ext.y * 0.5f * P4.w));
+    const float4 cpx = P1 - P4 * (from.x + ext.x * 0.5f + dx);
+    const float4 cpy = P2 - P4 * (from.y + ext.y * 0.5f + dy);
+    float4 ps;
+    float c = max_contrib_plane(cpx, P1, P2, P3, P4, ps);
+    if (c < best && in_screen_range(ps.y, from.y, ext.y, ps.w) && in_screen_range(ps.z, from.z, ext.z, ps.w)) best = c;
+    c = max_contrib_plane(cpy, P1, P2, P3, P4, ps);
+    if (c < best && in_screen_range(ps.x, from.x, ext.x, ps.w) && in_screen_range(ps.z, from.z, ext.z, ps.w)) best = c;
+    c = max_contrib_ray(cpx, cpy, P1, P2, P3, P4, ps);
+    if (c < best && in_screen_range(ps.z, from.z, ext.z, ps.w)) best = c;
+    const float4 opy = P2 - P4 * (from.y + ext.y * 0.5f - dy);
+    c = max_contrib_ray(cpx, opy, P1, P2, P3, P4, ps);
+    if (c < best && in_screen_range(ps.z, from.z, ext.z, ps.w)) best = c;
+    const float4 opx = P1 - P4 * (from.x + ext.x * 0.5f - dx);
+    c = max_contrib_ray(opx, cpy, P1, P2, P3, P4, ps);
+    if (c < best && in_screen_range(ps.z, from.z, ext.z, ps.w)) best = c;
+    return best;
+}
+__device__ __forceinline__ float normalize_angle(float th) {
+    constexpr float pi = 3.141592654f;
+    constexpr float two_pi = 2.0f * pi;
+    th = fmodf(th, two_pi);
+    if (th > pi) th -= two_pi;
+    if (th <= -pi) th += two_pi;
+    return th;
+}
+__device__ __forceinline__ float2 aabb_theta(float4 MT_axis, float4 MT3, float4 t, float theta_mu) {
+    constexpr float pi = 3.141592654f;
+    constexpr float two_pi = 2.0f * pi;
+    constexpr float max_theta = 0.5f * pi - 1e-5f;
+    const float sq_axis = dot(t, MT_axis * MT_axis);
+    const float sq_z = dot(t, MT3 * MT3);
+    const float mid = dot(t, MT_axis * MT3);
+    const float inside = mid * mid - sq_z * sq_axis;
+    float2 r = make_float2(-max_theta, max_theta);
+    if (inside > 0.0f) {
+        float2 th = make_float2(atan2f(-(mid + sqrtf(inside)), -sq_z), atan2f(-(mid - sqrtf(inside)), -sq_z));
+        while (th.x > theta_mu) th.x -= pi;
+        while (th.x < (theta_mu - pi)) th.x += pi;
+        while (th.y < theta_mu) th.y += pi;
+        while (th.y > (theta_mu + pi)) th.y -= pi;
+        const float2 tn = make_float2(normalize_angle(th.x), normalize_angle(th.y));
+        if (theta_mu < 0.0f && fabsf(tn.x) < fabsf(tn.y)) { th.x += two_pi; th.y += two_pi; }
+        else if (theta_mu > 0.0f && fabsf(tn.y) < fabsf(tn.x)) { th.x -= two_pi; th.y -= two_pi; }
+        r = make_float2(fmaxf(r.x, th.x), fminf(r.y, th.y));
+    }
+    return make_float2(tanf(r.x), tanf(r.y));
+}
+
+__device__ __forceinline__ bool transform_and_cull_aaa(const ViewParams& vp, const FrameParams& fp, float3 pos,
+                                                       float3 osc, float4 quat, float& opacity, float4& P1,
+                                                       float4& P2, float4& P4, uint4& b, uint32_t& n) {
+    const Mat3 R = quat_to_rot(quat);
+    const float4 M3 = vp.M[2];
+    const float z = dot(xyz(M3), pos) + M3.w;
+    constexpr float kernel_size = 0.3f;
+    const float max_focal = fmaxf(vp.focal_x, vp.focal_y);
+    const float fsv = z / max_focal;
+    const float fvar = fsv * fsv * kernel_size;
+    const float3 ovar = osc * osc;
+    const float3 var = make_float3(ovar.x + fvar, ovar.y + fvar, ovar.z + fvar);
+    const float3 sc = make_float3(sqrtf(var.x), sqrtf(var.y), sqrtf(var.z));
+    const float3 cam = xyz(vp.cam);
+    const float3 vdw = normalize(pos - cam);
+    const float3 vdg = make_float3(R.r11 * vdw.x + R.r21 * vdw.y + R.r31 * vdw.z,
+                                   R.r12 * vdw.x + R.r22 * vdw.y + R.r32 * vdw.z,
+                                   R.r13 * vdw.x + R.r23 * vdw.y + R.r33 * vdw.z);
+    const float3 r = vdg * vdg;
+    const float det_o = dot(r, make_float3(ovar.y * ovar.z, ovar.z * ovar.x, ovar.x * ovar.y));
+    const float det_d = dot(r, make_float3(var.y * var.z, var.z * var.x, var.x * var.y));
+    const float dil = sqrtf(__saturatef(det_o / det_d));
+    opacity *= dil;
+    if (opacity < kMinAlpha) return true;
+    const float rho_cutoff = 2.0f * logf(opacity * kMinAlphaRcp);
+    const float3 cs = cam - pos;
+    const float3 cg = make_float3(R.r11 * cs.x + R.r21 * cs.y + R.r31 * cs.z, R.r12 * cs.x + R.r22 * cs.y + R.r32 * cs.z,
+                                  R.r13 * cs.x + R.r23 * cs.y + R.r33 * cs.z) / sc;
+    if (dot(cg, cg) < rho_cutoff) return true;
+    const float3 u = make_float3(R.r11 * sc.x, R.r21 * sc.x, R.r31 * sc.x) * fp.scale_modifier;
+    const float3 v = make_float3(R.r12 * sc.y, R.r22 * sc.y, R.r32 * sc.y) * fp.scale_modifier;
+    const float3 w = make_float3(R.r13 * sc.z, R.r23 * sc.z, R.r33 * sc.z) * fp.scale_modifier;
+    P1 = xform_row(vp.VPM[0], u, v, w, pos);
+    P2 = xform_row(vp.VPM[1], u, v, w, pos);
+    const float4 P3 = xform_row(vp.VPM[2], u, v, w, pos);
+    P4 = xform_row(vp.VPM[3], u, v, w, pos);
+    const float mc = max_contrib_frustum(P1, P2, P3, P4, static_cast<float>(vp.width), static_cast<float>(vp.height));
+    if (mc > rho_cutoff) return true;
+    const float4 MT1 = xform_row(vp.M[0], u, v, w, pos);
+    const float4 MT2 = xform_row(vp.M[1], u, v, w, pos);
+    const float4 t = make_float4(rho_cutoff, rho_cutoff, rho_cutoff, -1.0f);
+    const float3 viewdir = normalize(make_float3(MT1.w, MT2.w, P4.w));
+    const float2 tx = aabb_theta(MT1, P4, t, atan2f(viewdir.x, viewdir.z));
+    const float2 ty = aabb_theta(MT2, P4, t, atan2f(viewdir.y, viewdir.z));
+    const float2 bxx = make_float2(vp.center_x + vp.focal_x * tx.x, vp.center_x + vp.focal_x * tx.y);
+    const float2 byy = make_float2(vp.center_y + vp.focal_y * ty.x, vp.center_y + vp.focal_y * ty.y);
+    const float2 ctr = make_float2((bxx.y + bxx.x) / 2.0f, (byy.y + byy.x) / 2.0f);
+    const float2 ext = make_float2((bxx.y - bxx.x) / 2.0f, (byy.y - byy.x) / 2.0f);
+    const uint32_t gw = static_cast<uint32_t>(vp.glw), gh = static_cast<uint32_t>(vp.glh);
+    const float tw = static_cast<float>(kTileLarge);
+    b = make_uint4(min(gw, static_cast<uint32_t>(max(0, __float2int_rd((ctr.x - ext.x) / tw)))),
+                   min(gw, static_cast<uint32_t>(max(0, __float2int_ru((ctr.x + ext.x) / tw)))),
+                   min(gh, static_cast<uint32_t>(max(0, __float2int_rd((ctr.y - ext.y) / tw)))),
+                   min(gh, static_cast<uint32_t>(max(0, __float2int_ru((ctr.y + ext.y) / tw)))));
+    n = touched_from_bounds(vp, b);
+    return n == 0;
+}
+
+__global__ void __launch_bounds__(kPrimBlock) preprocess_kernel(FrameParams fp, FrameBuffers fb, Gaussians g) {
+    __shared__ uint32_t s_warp[33];
+    const int i = blockIdx.x * kPrimBlock + threadIdx.x;
+    const bool valid = i < fp.n_prims;
+    const int ii = valid ? i : 0;
+    float3 pos = make_float3(0.f, 0.f, 0.f), scale = pos;
+    float4 quat = make_float4(1.f, 0.f, 0.f, 0.f);
+    float op = 0.0f;
+    if (valid) {
+        pos = ld3(g.positions + 3 * static_cast<size_t>(ii));
+        scale = ld3(g.scales + 3 * static_cast<size_t>(ii));
+        quat = ld4(g.rotations + 4 * static_cast<size_t>(ii));
+        op = g.opacities[ii];
+    }
+    const size_t N = static_cast<size_t>(fp.n_prims);
+    for (int v = 0; v < fp.n_views; ++v) {
+        const ViewParams& vp = fb.views[v];
+        uint32_t n = 0;
+        if (valid) {
+            float4 P1, P2, P4;
+            uint4 b;
+            float opacity = op;
+            const bool culled = fp.aaa ? transform_and_cull_aaa(vp, fp, pos, scale, quat, opacity, P1, P2, P4, b, n)
+                                       : transform_and_cull(vp, fp, pos, scale, quat, opacity, P1, P2, P4, b, n);
+            if (culled) n = 0;
+            const size_t o = static_cast<size_t>(v) * N + ii;
+            fb.n_touched[o] = n;
+            if (!culled) {
+                fb.bounds[o] = make_ushort4(static_cast<unsigned short>(b.x), static_cast<unsigned short>(b.y),
+                                            static_cast<unsigned short>(b.z), static_cast<unsigned short>(b.w));
+                const float3 rgb = sh_to_rgb(g.sh_0 + 3 * static_cast<size_t>(ii),
+                                             g.sh_rest + static_cast<size_t>(3) * fp.total_sh * ii, pos, xyz(vp.cam),
+                                             fp.active_sh);
+                float4* r = fb.rec + 4 * o;
+                r[0] = P1;
+                r[1] = P2;
+                r[2] = P4;
+                r[3] = make_float4(rgb.x, rgb.y, rgb.z, opacity);
+            }
+        }
+        uint32_t tot;
+        block_excl_scan<uint32_t>(n, tot, s_warp);
+        if (threadIdx.x == 0) fb.block_sums[static_cast<size_t>(v) * fp.n_blocks_prim + blockIdx.x] = tot;
+    }
+}
+
+int launch_preprocess(const FrameParams& fp, const FrameBuffers& fb, const Gaussians& g, cudaStream_t s) {
+    if (fp.n_blocks_prim == 0) return 0;
+    preprocess_kernel<<<fp.n_blocks_prim, kPrimBlock, 0, s>>>(fp, fb, g);
+    return 1;
+}
+
+// ------------------------------------------------------------------------------------------
+// scan of block sums -> block prefixes (in place) and M per view
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) scan_blocks_kernel(FrameParams fp, FrameBuffers fb) {
+    __shared__ unsigned long long s_warp[33];
+    const int v = blockIdx.x;
+    uint32_t* bs = fb.block_sums + static_cast<size_t>(v) * fp.n_blocks_prim;
+    const int nb = fp.n_blocks_prim;
+    unsigned long long carry = 0;
+    for (int base = 0; base < nb; base += blockDim.x) {
+        const int k = base + threadIdx.x;
+        const unsigned long long x = k < nb ? bs[k] : 0ull;
+        unsigned long long tot;
+        const unsigned long long e = block_excl_scan<unsigned long long>(x, tot, s_warp);
+        if (k < nb) bs[k] = static_cast<uint32_t>(carry + e);  // 32-bit offsets, as the reference
+        carry += tot;
+    }
+    if (threadIdx.x == 0) {
+        fb.status[v].n_instances = static_cast<uint32_t>(carry);
+        fb.status[v].overflow = static_cast<uint32_t>(carry) > static_cast<unsigned long long>(fp.cap) ? 1u : 0u;
+    }
+}
+
+int launch_scan_blocks(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s) {
+    scan_blocks_kernel<<<fp.n_views, 1024, 0, s>>>(fp, fb);
+    return 1;
+}
+
+// ------------------------------------------------------------------------------------------
+// instance creation (restates create_instances_cu, shared_kernels.cuh:15-130: keys
+// tile*4 (+sub-tile for fovea tiles) in row-major bbox order, values = primitive index; the
+// slots the area tables over-count keep the sentinel key, as the reference's 0xFF memset)
+// ------------------------------------------------------------------------------------------
+constexpr uint32_t kSeqTiles = 16;   // bbox tiles handled by the owning thread
+constexpr int kBigList = kPrimBlock;
+
+template <typename KeyT>
+__device__ __forceinline__ void emit(KeyT* keys, uint32_t* vals, uint64_t pos, uint64_t lim, KeyT key, uint32_t val) {
+    if (pos < lim) { keys[pos] = key; vals[pos] = val; }
+}
+
+template <typename KeyT>
+__global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParams fp, FrameBuffers fb) {
+    __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_big_n;
+    __shared__ uint32_t s_big_prim[kBigList];
+    __shared__ uint32_t s_big_off[kBigList];
+    __shared__ uint32_t s_big_cnt[kBigList];
+    __shared__ ushort4 s_big_b[kBigList];
+    const int v = blockIdx.y;
+    const ViewParams& vp = fb.views[v];
+    const int i = blockIdx.x * kPrimBlock + threadIdx.x;
+    const size_t N = static_cast<size_t>(fp.n_prims);
+    const size_t o = static_cast<size_t>(v) * N + i;
+    const uint32_t nt = i < fp.n_prims ? fb.n_touched[o] : 0u;
+    uint32_t tot;
+    const uint32_t local = block_excl_scan<uint32_t>(nt, tot, s_warp);
+    const uint32_t off = fb.block_sums[static_cast<size_t>(v) * fp.n_blocks_prim + blockIdx.x] + local;
+    const uint64_t lim = static_cast<uint64_t>(fp.cap);
+    KeyT* keys = reinterpret_cast<KeyT*>(fb.keys[0]) + static_cast<size_t>(v) * fp.cap;
+    uint32_t* vals = fb.vals[0] + static_cast<size_t>(v) * fp.cap;
+    const KeyT sentinel = static_cast<KeyT>(~KeyT(0));
+    const uint32_t glw = static_cast<uint32_t>(vp.glw);
+    if (threadIdx.x == 0) s_big_n = 0;
+    __syncthreads();
+    ushort4 b = make_ushort4(0, 0, 0, 0);
+    if (nt > 0) {
+        b = fb.bounds[o];
+        const uint32_t bw = static_cast<uint32_t>(b.y - b.x);
+        const uint32_t cnt = static_cast<uint32_t>(b.w - b.z) * bw;
+        if (cnt <= kSeqTiles) {
+            uint64_t w = off;
+            const uint64_t end = static_cast<uint64_t>(off) + nt;
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const uint32_t tx = b.x + k % bw, ty = b.z + k / bw;
+                const uint32_t tile = ty * glw + tx;
+                if (!tile_visible(vp.vis_mask, tile)) continue;
+                const KeyT key = static_cast<KeyT>(tile * kSubTiles);
+                if (in_fovea<kFoveaRadiusTiles>(tx, ty, vp.gaze_tiles)) {
+                    for (int r = 0; r < kSubTiles; ++r, ++w)
+                        if (w < end) emit<KeyT>(keys, vals, w, lim, static_cast<KeyT>(key + r), static_cast<uint32_t>(i));
+                } else {
+                    if (w < end) emit<KeyT>(keys, vals, w, lim, key, static_cast<uint32_t>(i));
+                    ++w;
+                }
+            }
+            for (; w < end; ++w) emit<KeyT>(keys, vals, w, lim, sentinel, static_cast<uint32_t>(i));
+        } else {
+            const uint32_t slot = atomicAdd(&s_big_n, 1u);
+            s_big_prim[slot] = static_cast<uint32_t>(i);
+            s_big_off[slot] = off;
+            s_big_cnt[slot] = nt;
+            s_big_b[slot] = b;
+        }
+    }
+    __syncthreads();
+    // Large footprints: the whole block walks the bounding box, 256 tiles per step, with a
+    // block scan of the per-tile instance counts giving each tile's slots.
+    const uint32_t n_big = s_big_n;
+    for (uint32_t q = 0; q < n_big; ++q) {
+        const uint32_t prim = s_big_prim[q];
+        const ushort4 bb = s_big_b[q];
+        const uint32_t bw = static_cast<uint32_t>(bb.y - bb.x);
+        const uint32_t cnt = static_cast<uint32_t>(bb.w - bb.z) * bw;
+        const uint64_t end = static_cast<uint64_t>(s_big_off[q]) + s_big_cnt[q];
+        uint64_t w0 = s_big_off[q];
+        for (uint32_t base = 0; base < cnt; base += kPrimBlock) {
+            const uint32_t k = base + threadIdx.x;
+            uint32_t c = 0, tile = 0;
+            bool fov = false;
+            if (k < cnt) {
+                const uint32_t tx = bb.x + k % bw, ty = bb.z + k / bw;
+                tile = ty * glw + tx;
+                if (tile_visible(vp.vis_mask, tile)) {
+                    fov = in_fovea<kFoveaRadiusTiles>(tx, ty, vp.gaze_tiles);
+                    c = fov ? kSubTiles : 1;
+                }
+            }
+            uint32_t step;
+            const uint32_t ex = block_excl_scan<uint32_t>(c, step, s_warp);
+            const KeyT key = static_cast<KeyT>(tile * kSubTiles);
+            for (uint32_t r = 0; r < c; ++r) {
+                const uint64_t w = w0 + ex + r;
+                if (w < end) emit<KeyT>(keys, vals, w, lim, static_cast<KeyT>(key + r), prim);
+            }
+            w0 += step;
+        }
+        for (uint64_t w = w0 + threadIdx.x; w < end; w += kPrimBlock) emit<KeyT>(keys, vals, w, lim, sentinel, prim);
+    }
+}
+
+int launch_create(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s) {
+    if (fp.n_blocks_prim == 0) return 0;
+    dim3 grid(fp.n_blocks_prim, fp.n_views);
+    if (fp.key_u32) create_instances_kernel<uint32_t><<<grid, kPrimBlock, 0, s>>>(fp, fb);
+    else create_instances_kernel<uint16_t><<<grid, kPrimBlock, 0, s>>>(fp, fb);
+    return 1;
+}
+
+// ------------------------------------------------------------------------------------------
+// stable LSD radix sort of (key, value) pairs per view (replaces cub::DeviceRadixSort::
+// SortPairs over bits [0, end_bit), inference.cu:267-274).  Digit ranking with
+// __match_any_sync per warp; counts per (digit, tile) scanned digit-major; the scatter goes
+// through shared memory so that global stores run along digit runs.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t view_count(const FrameParams& fp, const FrameBuffers& fb, int v) {
+    const unsigned long long m = fb.status[v].n_instances;
+    return m < static_cast<unsigned long long>(fp.cap) ? m : static_cast<unsigned long long>(fp.cap);
+}
+
+template <typename KeyT>
+__global__ void __launch_bounds__(kSortThreads) sort_upsweep_kernel(FrameParams fp, FrameBuffers fb, int buf, int shift) {
+    __shared__ uint32_t s_hist[kSortThreads / 32][kSortBins];
+    const int v = blockIdx.y;
+    const uint64_t M = view_count(fp, fb, v);
+    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kSortTile;
+    if (t0 >= M) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = threadIdx.x; k < (kSortThreads / 32) * kSortBins; k += kSortThreads) (&s_hist[0][0])[k] = 0;
+    __syncthreads();
+    const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[buf]) + static_cast<size_t>(v) * fp.cap;
+    const uint64_t wbase = t0 + static_cast<uint64_t>(warp) * 32 * kSortItems;
+#pragma unroll 4
+    for (int it = 0; it < kSortItems; ++it) {
+        const uint64_t idx = wbase + static_cast<uint64_t>(it) * 32 + lane;
+        const bool ok = idx < M;
+        const uint32_t d = ok ? (static_cast<uint32_t>(keys[idx]) >> shift) & (kSortBins - 1) : kSortBins;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        if (ok && lane == __ffs(peers) - 1) s_hist[warp][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    const int d = threadIdx.x;  // kSortThreads == kSortBins
+    uint32_t c = 0;
+#pragma unroll
+    for (int w = 0; w < kSortThreads / 32; ++w) c += s_hist[w][d];
+    fb.sort_hist[(static_cast<size_t>(v) * kSortBins + d) * fb.sort_tiles + blockIdx.x] = c;
+}
+
+__global__ void __launch_bounds__(256) sort_scan_kernel(FrameParams fp, FrameBuffers fb) {
+    __shared__ uint32_t s_warp[33];
+    const int d = blockIdx.x, v = blockIdx.y;
+    const uint64_t M = view_count(fp, fb, v);
+    const int ntiles = static_cast<int>((M + kSortTile - 1) / kSortTile);
+    uint32_t* row = fb.sort_hist + (static_cast<size_t>(v) * kSortBins + d) * fb.sort_tiles;
+    uint32_t carry = 0;
+    for (int base = 0; base < ntiles; base += blockDim.x) {
+        const int k = base + threadIdx.x;
+        const uint32_t x = k < ntiles ? row[k] : 0u;
+        uint32_t tot;
+        const uint32_t e = block_excl_scan<uint32_t>(x, tot, s_warp);
+        if (k < ntiles) row[k] = carry + e;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) fb.sort_digit_tot[static_cast<size_t>(v) * kSortBins + d] = carry;
+}
+
+template <typename KeyT>
+__global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(FrameParams fp, FrameBuffers fb, int buf, int shift) {
+    __shared__ uint32_t s_whist[kSortThreads / 32][kSortBins];  // per-warp counts -> per-warp prefix
+    __shared__ uint32_t s_local_start[kSortBins];
+    __shared__ uint32_t s_global_start[kSortBins];
+    __shared__ uint32_t s_warp[33];
+    __shared__ KeyT s_keys[kSortTile];
+    __shared__ uint32_t s_vals[kSortTile];
+    const int v = blockIdx.y;
+    const uint64_t M = view_count(fp, fb, v);
+    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kSortTile;
+    if (t0 >= M) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lanemask_lt = (1u << lane) - 1u;
+    for (int k = threadIdx.x; k < (kSortThreads / 32) * kSortBins; k += kSortThreads) (&s_whist[0][0])[k] = 0;
+    __syncthreads();
+    const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[buf]) + static_cast<size_t>(v) * fp.cap;
+    const uint32_t* vals = fb.vals[buf] + static_cast<size_t>(v) * fp.cap;
+    KeyT* okeys = reinterpret_cast<KeyT*>(fb.keys[buf ^ 1]) + static_cast<size_t>(v) * fp.cap;
+    uint32_t* ovals = fb.vals[buf ^ 1] + static_cast<size_t>(v) * fp.cap;
+    const uint64_t wbase = t0 + static_cast<uint64_t>(warp) * 32 * kSortItems;
+    KeyT k_reg[kSortItems];
+    uint32_t v_reg[kSortItems];
+    uint32_t rank[kSortItems];
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+        const uint64_t idx = wbase + static_cast<uint64_t>(it) * 32 + lane;
+        const bool ok = idx < M;
+        k_reg[it] = ok ? keys[idx] : static_cast<KeyT>(0);
+        v_reg[it] = ok ? vals[idx] : 0u;
+        const uint32_t d = ok ? (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1) : kSortBins;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t before = ok ? s_whist[warp][d] : 0u;
+        rank[it] = before + __popc(peers & lanemask_lt);
+        __syncwarp();
+        if (ok && lane == __ffs(peers) - 1) s_whist[warp][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // per-digit: exclusive prefix over warps, tile count, local start (scan over digits)
+    const int d = threadIdx.x;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int w = 0; w < kSortThreads / 32; ++w) {
+        const uint32_t c = s_whist[w][d];
+        s_whist[w][d] = cnt;
+        cnt += c;
+    }
+    uint32_t tile_total;
+    const uint32_t lstart = block_excl_scan<uint32_t>(cnt, tile_total, s_warp);
+    s_local_start[d] = lstart;
+    // global start of digit d for this tile: exclusive scan of digit totals + tile offset
+    const uint32_t dtot = fb.sort_digit_tot[static_cast<size_t>(v) * kSortBins + d];
+    uint32_t all_total;
+    const uint32_t dbase = block_excl_scan<uint32_t>(dtot, all_total, s_warp);
+    s_global_start[d] = dbase + fb.sort_hist[(static_cast<size_t>(v) * kSortBins + d) * fb.sort_tiles + blockIdx.x];
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+        const uint64_t idx = wbase + static_cast<uint64_t>(it) * 32 + lane;
+        if (idx < M) {
+            const uint32_t dd = (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1);
+            const uint32_t p = s_local_start[dd] + s_whist[warp][dd] + rank[it];
+            s_keys[p] = k_reg[it];
+            s_vals[p] = v_reg[it];
+        }
+    }
+    __syncthreads();
+    const uint32_t n_here = static_cast<uint32_t>(M - t0 < static_cast<uint64_t>(kSortTile) ? M - t0 : kSortTile);
+    for (uint32_t j = threadIdx.x; j < n_here; j += kSortThreads) {
+        const KeyT kk = s_keys[j];
+        const uint32_t dd = (static_cast<uint32_t>(kk) >> shift) & (kSortBins - 1);
+        const uint32_t gpos = s_global_start[dd] + (j - s_local_start[dd]);
+        okeys[gpos] = kk;
+        ovals[gpos] = s_vals[j];
+    }
+}
+
+template <typename KeyT>
+int sort_t(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s) {
+    const int passes = (fp.end_bit + kSortRadixBits - 1) / kSortRadixBits;
+    int buf = 0;
+    dim3 gt(fb.sort_tiles, fp.n_views), gd(kSortBins, fp.n_views);
+    for (int p = 0; p < passes; ++p) {
+        const int shift = p * kSortRadixBits;
+        sort_upsweep_kernel<KeyT><<<gt, kSortThreads, 0, s>>>(fp, fb, buf, shift);
+        sort_scan_kernel<<<gd, 256, 0, s>>>(fp, fb);
+        sort_scatter_kernel<KeyT><<<gt, kSortThreads, 0, s>>>(fp, fb, buf, shift);
+        buf ^= 1;
+    }
+    fb.final_buf = buf;
+    return 3 * passes;
+}
+
+int launch_sort(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s) {
+    if (fb.sort_tiles == 0) { fb.final_buf = 0; return 0; }
+    return fp.key_u32 ? sort_t<uint32_t>(fp, fb, s) : sort_t<uint16_t>(fp, fb, s);
+}
+
+// ------------------------------------------------------------------------------------------
+// per-small-tile instance ranges (restates extract_instance_ranges_cu,
+// shared_kernels.cuh:133-152; ranges are zeroed beforehand)
+// ------------------------------------------------------------------------------------------
+template <typename KeyT>
+__global__ void ranges_kernel(FrameParams fp, FrameBuffers fb) {
+    const int v = blockIdx.y;
+    const uint64_t M = view_count(fp, fb, v);
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[fb.final_buf]) + static_cast<size_t>(v) * fp.cap;
+    uint2* r = fb.ranges + static_cast<size_t>(v) * fp.max_tiles;
+    const KeyT sentinel = static_cast<KeyT>(~KeyT(0));
+    const KeyT k = keys[i];
+    if (i == 0) {
+        if (k != sentinel) r[k].x = 0;
+    } else {
+        const KeyT prev = keys[i - 1];
+        if (k != prev) {
+            if (prev != sentinel) r[prev].y = static_cast<uint32_t>(i);
+            if (k != sentinel) r[k].x = static_cast<uint32_t>(i);
+        }
+    }
+    if (i == M - 1 && k != sentinel) r[k].y = static_cast<uint32_t>(M);
+}
+
+int launch_ranges(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s) {
+    cudaMemsetAsync(fb.ranges, 0, sizeof(uint2) * static_cast<size_t>(fp.max_tiles) * fp.n_views, s);
+    if (fb.sort_tiles == 0) return 0;
+    const unsigned nb = static_cast<unsigned>((fp.cap + 255) / 256);
+    dim3 grid(nb, fp.n_views);
+    if (fp.key_u32) ranges_kernel<uint32_t><<<grid, 256, 0, s>>>(fp, fb);
+    else ranges_kernel<uint16_t><<<grid, 256, 0, s>>>(fp, fb);
+    return 1;
+}
+
+// ------------------------------------------------------------------------------------------
+// K-buffer blend (restates blend_cu and FragmentInfo, inference.cuh:16-286, and the
+// background models, background_model.cuh:8-117).  Per pixel the arithmetic and the order of
+// Gaussians are the reference's; a Gaussian is skipped for a whole warp when the warp's pixel
+// rectangle lies outside the Gaussian's cutoff ellipse bounding box (+1 px), where every pixel
+// would fail the alpha >= 1/255 test anyway.
+// ------------------------------------------------------------------------------------------
+struct Frag {
+    float depth;
+    uint32_t color;
+};
+
+__device__ __forceinline__ uint32_t pack_channel(const float x) {
+    return static_cast<uint32_t>(fminf(fmaxf(x, 0.0f), 1.0f) * 255.0f + 0.5f);
+}
+__device__ __forceinline__ uint32_t pack_rgba(const float4 c) {
+    return pack_channel(c.x) | (pack_channel(c.y) << 8) | (pack_channel(c.z) << 16) | (pack_channel(c.w) << 24);
+}
+__device__ __forceinline__ float4 unpack_rgba(const uint32_t c) {
+    return make_float4(static_cast<float>((c >> 0) & 0xff), static_cast<float>((c >> 8) & 0xff),
+                       static_cast<float>((c >> 16) & 0xff), static_cast<float>((c >> 24) & 0xff)) * (1.0f / 255.0f);
+}
+
+__device__ __forceinline__ float3 background_dir(const ViewParams& vp, float px, float py) {
+    const float4 pc = make_float4(px, py, 1.0f, 1.0f);
+    return normalize(make_float3(dot(vp.VPR_inv[0], pc), dot(vp.VPR_inv[1], pc), dot(vp.VPR_inv[2], pc)));
+}
+
+__device__ float3 eval_sh_background(const ViewParams& vp, const float* __restrict__ c, float px, float py) {
+    const float3 t = background_dir(vp, px, py);
+    if (t.y > 0.1f) return make_float3(0.0f, 0.0f, 0.0f);
+    const float3 n = normalize(t);
+    const float x = n.x, y = n.y, z = n.z;
+    const float xx = x * x, yy = y * y, zz = z * z;
+    const float xy = x * y, xz = x * z, yz = y * z;
+    const float3 e = 0.5f + kC0 * ld3(c + 0) - kC1 * y * ld3(c + 3) + kC1 * z * ld3(c + 6) - kC1 * x * ld3(c + 9)
+                     + kC2a * xy * ld3(c + 12) - kC2a * yz * ld3(c + 15) + (kC2b * zz - kC2c) * ld3(c + 18)
+                     - kC2a * xz * ld3(c + 21) + kC2d * (xx - yy) * ld3(c + 24)
+                     + y * (kC3a * yy - kC3b * xx) * ld3(c + 27) + kC3c * xy * z * ld3(c + 30)
+                     + y * (kC3d - kC3e * zz) * ld3(c + 33) + z * (kC3f * zz - kC3g) * ld3(c + 36)
+                     + x * (kC3d - kC3e * zz) * ld3(c + 39) + kC3h * z * (xx - yy) * ld3(c + 42)
+                     + x * (kC3b * yy - kC3a * xx) * ld3(c + 45);
+    const float3 col = make_float3(__saturatef(tanhf(e.x) * 0.5f + 0.5f), __saturatef(tanhf(e.y) * 0.5f + 0.5f),
+                                   __saturatef(tanhf(e.z) * 0.5f + 0.5f));
+    return t.y > 0.0f ? (1.0f - t.y / 0.1f) * col : col;
+}
+
+__device__ float3 eval_tex_background(const ViewParams& vp, const float* __restrict__ tex, int W, int H, bool act,
+                                      float px, float py) {
+    const float3 t = background_dir(vp, px, py);
+    if (t.y > 0.1f) return make_float3(0.0f, 0.0f, 0.0f);
+    constexpr float kPi = 3.14159265358979323846f;
+    const float2 eq = make_float2(atan2f(t.x, t.z) / kPi * 0.5f + 0.5f, asinf(t.y) / (0.5f * kPi) * 0.5f + 0.5f);
+    const float tx = eq.x * W - 0.5f;
+    const float ty = eq.y * H - 0.5f;
+    const int x0 = __float2int_rd(tx), y0 = __float2int_rd(ty);
+    const int x1 = x0 + 1, y1 = y0 + 1;
+    const float fx = tx - x0, fy = ty - y0;
+    const int x0w = x0 < 0 ? x0 + W : x0, x1w = x1 >= W ? x1 - W : x1;
+    const int y0c = max(0, min(H - 1, y0)), y1c = max(0, min(H - 1, y1));
+    const int i00 = x0w + y0c * W, i10 = x1w + y0c * W, i01 = x0w + y1c * W, i11 = x1w + y1c * W;
+    const int nt = W * H;
+    float3 col = make_float3(0.0f, 0.0f, 0.0f);
+    for (int ch = 0; ch < 3; ++ch) {
+        const int off = ch * nt;
+        const float c00 = tex[i00 + off], c10 = tex[i10 + off], c01 = tex[i01 + off], c11 = tex[i11 + off];
+        const float c0 = c00 * (1.0f - fx) + c10 * fx;
+        const float c1 = c01 * (1.0f - fx) + c11 * fx;
+        float cc = c0 * (1.0f - fy) + c1 * fy;
+        if (act) cc = 1.0f / (1.0f + __expf(-cc));
+        if (ch == 0) col.x = cc; else if (ch == 1) col.y = cc; else col.z = cc;
+    }
+    return t.y > 0.0f ? (1.0f - t.y / 0.1f) * col : col;
+}
+
+__device__ __forceinline__ void store_rgb(float* img, int W, int H, int x, int y, bool chw, float r, float g, float b) {
+    const int p = W * y + x;
+    if (chw) {
+        const int n = W * H;
+        img[p] = r;
+        img[n + p] = g;
+        img[2 * n + p] = b;
+    } else {
+        img[3 * p] = r;
+        img[3 * p + 1] = g;
+        img[3 * p + 2] = b;
+    }
+}
+
+// Pixel-space bounding box of a Gaussian's cutoff ellipse, evaluated about the projected
+// mean (x0 = P1.w / P4.w) so that no large terms cancel.  Returns false when the box is
+// unbounded (camera inside the cutoff quadric or mean behind it): no culling then.
+__device__ __forceinline__ bool cutoff_box(const float4 P1, const float4 P2, const float4 P4, float opacity,
+                                           float4& box, bool& never) {
+    never = false;
+    const float rc = 2.0f * __logf(opacity * kMinAlphaRcp);
+    if (rc < 0.0f) { never = true; return true; }  // alpha <= opacity < 1/255 everywhere
+    if (!(P4.w > 0.0f) || !(rc > 0.0f)) return false;
+    const float3 n4 = xyz(P4);
+    const float a = P4.w * P4.w - rc * dot(n4, n4);
+    if (!(a > 0.0f)) return false;
+    const float ia = 1.0f / a;
+    const float x0 = P1.w / P4.w, y0 = P2.w / P4.w;
+    const float3 q1 = xyz(P1) - x0 * n4, q2 = xyz(P2) - y0 * n4;
+    const float cx = -rc * dot(q1, n4) * ia, cy = -rc * dot(q2, n4) * ia;
+    const float ex = sqrtf(fmaxf(cx * cx + rc * dot(q1, q1) * ia, 0.0f));
+    const float ey = sqrtf(fmaxf(cy * cy + rc * dot(q2, q2) * ia, 0.0f));
+    if (!(isfinite(ex) && isfinite(ey) && isfinite(x0) && isfinite(y0))) return false;
+    const float mx = 1.0f + 1e-4f * (fabsf(x0) + ex), my = 1.0f + 1e-4f * (fabsf(y0) + ey);
+    box = make_float4(x0 + cx - ex - mx, x0 + cx + ex + mx, y0 + cy - ey - my, y0 + cy + ey + my);
+    return true;
+}
+
+// One block renders one 16x16 area.  LOWRES: 64 threads sample it at stride 2 (periphery);
+// otherwise 256 threads render it at full resolution (fovea / blended).  Warp w covers an
+// 8-wide, 4-high block of samples.
+template <int K, bool LOWRES>
+__global__ void __launch_bounds__(LOWRES ? 64 : 256) blend_kernel(FrameParams fp, FrameBuffers fb, int counter_idx) {
+    constexpr int NT = LOWRES ? 64 : 256;
+    constexpr int NW = NT / 32;
+    constexpr int S = LOWRES ? kStride : 1;
+    __shared__ float4 s_p1[NT], s_p2[NT], s_p4[NT], s_rgba[NT];
+    __shared__ uint32_t s_mask[NT];
+    __shared__ int s_item;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int lx = (warp & 1) * 8 + (lane & 7);
+    const int ly = (warp >> 1) * 4 + (lane >> 3);
+    // total work items over all views
+    int total = 0;
+    for (int v = 0; v < fp.n_views; ++v) {
+        const FrameStatus& st = fb.status[v];
+        total += LOWRES ? static_cast<int>(st.n_periphery_large) : static_cast<int>(st.n_fovea_large + st.n_blended_large);
+    }
+    for (;;) {
+        if (tid == 0) s_item = static_cast<int>(atomicAdd(&fb.counters[counter_idx], 1u));
+        __syncthreads();
+        int item = s_item;
+        __syncthreads();
+        if (item >= total) break;
+        int v = 0;
+        for (; v < fp.n_views; ++v) {
+            const FrameStatus& st = fb.status[v];
+            const int c = LOWRES ? static_cast<int>(st.n_periphery_large) : static_cast<int>(st.n_fovea_large + st.n_blended_large);
+            if (item < c) break;
+            item -= c;
+        }
+        const ViewParams& vp = fb.views[v];
+        const FrameStatus& st = fb.status[v];
+        const uint32_t lt = LOWRES ? fb.work_low[static_cast<size_t>(v) * fp.max_large + item]
+                                   : fb.work_full[static_cast<size_t>(v) * fp.max_large + item];
+        const bool is_fovea = !LOWRES && static_cast<uint32_t>(item) < st.n_fovea_large;
+        const int ox = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)) * kTileLarge;
+        const int oy = static_cast<int>(lt / static_cast<uint32_t>(vp.glw)) * kTileLarge;
+        const int px_i = ox + lx * S, py_i = oy + ly * S;
+        const bool inside = px_i < vp.width && py_i < vp.height;
+        const float pixel_x = __uint2float_rn(static_cast<uint32_t>(px_i));
+        const float pixel_y = __uint2float_rn(static_cast<uint32_t>(py_i));
+        // warp rectangle in pixels
+        const float wx0 = static_cast<float>(ox + (warp & 1) * 8 * S), wx1 = wx0 + 7.0f * S;
+        const float wy0 = static_cast<float>(oy + (warp >> 1) * 4 * S), wy1 = wy0 + 3.0f * S;
+        const uint2 range = fb.ranges[static_cast<size_t>(v) * fp.max_tiles + lt * kSubTiles];
+        const uint32_t* vals = fb.vals[fb.final_buf] + static_cast<size_t>(v) * fp.cap;
+        const float4* rec = fb.rec + 4 * static_cast<size_t>(v) * fp.n_prims;
+
+        float tail_T = 1.0f;
+        float4 tail = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        Frag core[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) { core[k].depth = 3.402823466e+38f; core[k].color = 0u; }
+
+        for (uint32_t start = range.x; start < range.y; start += NT) {
+            const uint32_t n_batch = min(static_cast<uint32_t>(NT), range.y - start);
+            __syncthreads();
+            if (static_cast<uint32_t>(tid) < n_batch) {
+                const uint32_t p = vals[start + tid];
+                const float4* r = rec + 4 * static_cast<size_t>(p);
+                const float4 P1 = r[0], P2 = r[1], P4 = r[2], c = r[3];
+                s_p1[tid] = P1;
+                s_p2[tid] = P2;
+                s_p4[tid] = P4;
+                s_rgba[tid] = c;
+                float4 box;
+                bool never;
+                uint32_t m = (1u << NW) - 1u;
+                if (cutoff_box(P1, P2, P4, c.w, box, never)) {
+                    if (never) m = 0u;
+                    else {
+                        m = 0u;
+#pragma unroll
+                        for (int w = 0; w < NW; ++w) {
+                            const float ax0 = static_cast<float>(ox + (w & 1) * 8 * S), ax1 = ax0 + 7.0f * S;
+                            const float ay0 = static_cast<float>(oy + (w >> 1) * 4 * S), ay1 = ay0 + 3.0f * S;
+                            if (box.y >= ax0 && box.x <= ax1 && box.w >= ay0 && box.z <= ay1) m |= 1u << w;
+                        }
+                    }
+                }
+                s_mask[tid] = m;
+            }
+            __syncthreads();
+            (void)wx0; (void)wx1; (void)wy0; (void)wy1;
+            for (uint32_t j = 0; j < n_batch; ++j) {
+                if (!((s_mask[j] >> warp) & 1u)) continue;
+                if (!inside) continue;
+                const float4 VPMT1 = s_p1[j], VPMT2 = s_p2[j], VPMT4 = s_p4[j];
+                const float4 plane_x = VPMT1 - VPMT4 * pixel_x;
+                const float4 plane_y = VPMT2 - VPMT4 * pixel_y;
+                const float3 nx = xyz(plane_x), ny = xyz(plane_y);
+                const float3 m = plane_x.w * ny - nx * plane_y.w;
+                const float3 d = cross(nx, ny);
+                const float num = dot(m, m);
+                const float den = dot(d, d);
+                if (num > kMaxCutoffSq * den) continue;
+                const float den_rcp = 1.0f / den;
+                const float G = expf(-0.5f * num * den_rcp);
+                const float4 c = s_rgba[j];
+                const float alpha = fminf(c.w * G, kMaxFragmentAlpha);
+                if (alpha < kMinAlpha) continue;
+                const float3 ep = cross(d, m) * den_rcp;
+                const float depth = dot(xyz(VPMT4), ep) + VPMT4.w;
+                float4 pm = make_float4(c.x * alpha, c.y * alpha, c.z * alpha, alpha);
+                if (depth < core[K - 1].depth && alpha >= kMinAlphaCore) {
+                    Frag f;
+                    f.depth = depth;
+                    f.color = pack_rgba(pm);
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        if (f.depth < core[k].depth) {
+                            const Frag t = core[k];
+                            core[k] = f;
+                            f = t;
+                        }
+                    }
+                    pm = unpack_rgba(f.color);
+                }
+                const float pt = 1.0f - pm.w;
+                tail += pm;
+                tail_T *= pt;
+            }
+        }
+        if (inside) {
+            float3 rgb = make_float3(0.0f, 0.0f, 0.0f);
+            float Tc = 1.0f;
+#pragma unroll
+            for (int k = 0; k < K && Tc >= kTransmittanceThreshold; ++k) {
+                const float4 c = unpack_rgba(core[k].color);
+                rgb += Tc * xyz(c);
+                Tc *= 1.0f - c.w;
+            }
+            if (Tc >= kTransmittanceThreshold && tail.w >= kMinAlpha) {
+                const float wt = Tc * (1.0f - tail_T);
+                rgb += wt * (1.0f / tail.w) * xyz(tail);
+            }
+            if (fp.bg_type != 0) {
+                const float wb = Tc * tail_T;
+                if (wb >= kTransmittanceThreshold) {
+                    if (fp.bg_type == 1) rgb += wb * eval_sh_background(vp, fp.bg_data, pixel_x, pixel_y);
+                    else rgb += wb * eval_tex_background(vp, fp.bg_data, fp.tex_w, fp.tex_h, fp.bg_type == 3, pixel_x, pixel_y);
+                }
+            }
+            float* out = is_fovea ? vp.image : vp.work;
+            store_rgb(out, vp.width, vp.height, px_i, py_i, fp.to_chw != 0, __saturatef(rgb.x), __saturatef(rgb.y),
+                      __saturatef(rgb.z));
+        }
+    }
+}
+
+template <int K>
+int launch_blend_k(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid) {
+    static int occ_full = -1, occ_low = -1;  // per instantiation, queried once
+    if (occ_full < 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_full, blend_kernel<K, false>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_low, blend_kernel<K, true>, 64, 0);
+    }
+    const int gfull = n_sms * (occ_full > 0 ? occ_full : 1);
+    const int glow = n_sms * (occ_low > 0 ? occ_low : 1);
+    blend_kernel<K, false><<<gfull, 256, 0, s>>>(fp, fb, 0);
+    if (mid) cudaEventRecord(mid, s);
+    blend_kernel<K, true><<<glow, 64, 0, s>>>(fp, fb, 1);
+    return 2;
+}
+
+int launch_blend(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid) {
+    const int K = fp.K;
+    if (K >= 32) return launch_blend_k<32>(fp, fb, n_sms, s, mid);
+    if (K >= 16) return launch_blend_k<16>(fp, fb, n_sms, s, mid);
+    if (K >= 8) return launch_blend_k<8>(fp, fb, n_sms, s, mid);
+    if (K >= 4) return launch_blend_k<4>(fp, fb, n_sms, s, mid);
+    if (K >= 2) return launch_blend_k<2>(fp, fb, n_sms, s, mid);
+    return launch_blend_k<1>(fp, fb, n_sms, s, mid);
+}
+
+// ------------------------------------------------------------------------------------------
+// compose: periphery upsampling / blur and blended cross-fade (restates
+// bilinear_interpolation, bilinear_interpolation_blended, interpolate_and_blur and
+// interpolate_and_blur_blended, interpolation.cuh:11-584), plus clearing of masked tiles.
+// One 256-thread block per large tile; blended tiles use four 64-thread groups.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ float3 load_rgb(const float* img, int W, int H, int x, int y, bool chw) {
+    const int sx = clampi(x, 0, W - 1), sy = clampi(y, 0, H - 1);
+    const int p = W * sy + sx;
+    if (chw) {
+        const int n = W * H;
+        return make_float3(img[p], img[n + p], img[2 * n + p]);
+    }
+    return make_float3(img[3 * p], img[3 * p + 1], img[3 * p + 2]);
+}
+
+// Sample (sx, sy) of a stride-2 grid starting at (bx, by); masked-tile samples are clamped
+// into the large tile (ltx, lty).  `zero_fovea`: the blend target holds no fovea pixels
+// (blur mode), where the reference's zero-initialised temporary buffer reads as 0.
+__device__ __forceinline__ float3 grid_sample(const ViewParams& vp, const uint8_t* ltype, const float* src, bool chw,
+                                              int bx, int by, int sx, int sy, int max_r, int max_d, int ltx, int lty,
+                                              bool zero_fovea) {
+    const int px = bx + min(sx, max_r) * kStride;
+    const int py = by + min(sy, max_d) * kStride;
+    const int tile = py / kTileLarge * vp.glw + px / kTileLarge;
+    if ((vp.vis_mask[tile / 32] & (1u << (tile % 32))) == 0) {
+        const int cx = clampi(px, ltx * kTileLarge, ltx * kTileLarge + kTileLarge - kStride);
+        const int cy = clampi(py, lty * kTileLarge, lty * kTileLarge + kTileLarge - kStride);
+        return load_rgb(src, vp.width, vp.height, cx, cy, chw);
+    }
+    if (zero_fovea) {
+        const int qx = clampi(px, 0, vp.width - 1), qy = clampi(py, 0, vp.height - 1);
+        if (ltype[(qy / kTileLarge) * vp.glw + qx / kTileLarge] == kFovea) return make_float3(0.0f, 0.0f, 0.0f);
+    }
+    return load_rgb(src, vp.width, vp.height, px, py, chw);
+}
+
+__device__ __forceinline__ float3 bilerp(const float3* s, int n, int lx, int ly) {
+    const int bx = lx / kStride, by = ly / kStride;
+    const float xf = static_cast<float>(lx % kStride) / static_cast<float>(kStride);
+    const float yf = static_cast<float>(ly % kStride) / static_cast<float>(kStride);
+    float3 r = make_float3(0.0f, 0.0f, 0.0f);
+    if (lx % kStride == 0) {
+        r += s[by * n + bx] * (1.0f - yf);
+        r += s[(by + 1) * n + bx] * yf;
+    } else if (ly % kStride == 0) {
+        r += s[by * n + bx] * (1.0f - xf);
+        r += s[by * n + bx + 1] * xf;
+    } else {
+        r += s[by * n + bx] * (1.0f - xf) * (1.0f - yf);
+        r += s[by * n + bx + 1] * xf * (1.0f - yf);
+        r += s[(by + 1) * n + bx] * (1.0f - xf) * yf;
+        r += s[(by + 1) * n + bx + 1] * xf * yf;
+    }
+    return r;
+}
+
+__device__ __forceinline__ float3 blur5(const float3* s, int n, int lx, int ly, float& factor) {
+    const int bx = lx / 2 + 1, by = ly / 2 + 1;
+    auto S = [&](int yy, int xx) { return s[yy * n + xx]; };
+    float3 r = make_float3(0.0f, 0.0f, 0.0f);
+    if ((lx & 1) == 0 && (ly & 1) == 0) {
+        factor = 1.0f / 64.0f;
+        r += S(by - 1, bx - 1); r += S(by - 1, bx) * 6.0f; r += S(by - 1, bx + 1);
+        r += S(by, bx - 1) * 6.0f; r += S(by, bx) * 36.0f; r += S(by, bx + 1) * 6.0f;
+        r += S(by + 1, bx - 1); r += S(by + 1, bx) * 6.0f; r += S(by + 1, bx + 1);
+    } else if ((lx & 1) == 0 && (ly & 1) == 1) {
+        factor = 1.0f / 16.0f;
+        r += S(by, bx - 1); r += S(by, bx) * 6.0f; r += S(by, bx + 1);
+        r += S(by + 1, bx - 1); r += S(by + 1, bx) * 6.0f; r += S(by + 1, bx + 1);
+    } else if ((lx & 1) == 1 && (ly & 1) == 0) {
+        factor = 1.0f / 16.0f;
+        r += S(by - 1, bx); r += S(by - 1, bx + 1);
+        r += S(by, bx) * 6.0f; r += S(by, bx + 1) * 6.0f;
+        r += S(by + 1, bx); r += S(by + 1, bx + 1);
+    } else {
+        factor = 1.0f / 4.0f;
+        r += S(by, bx); r += S(by, bx + 1); r += S(by + 1, bx); r += S(by + 1, bx + 1);
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(256) compose_kernel(FrameParams fp, FrameBuffers fb) {
+    __shared__ float3 s_samples[4][10 * 10];
+    const int v = blockIdx.y;
+    const ViewParams& vp = fb.views[v];
+    const FrameStatus& st = fb.status[v];
+    const int nP = static_cast<int>(st.n_periphery_large), nB = static_cast<int>(st.n_blended_large),
+              nM = static_cast<int>(st.n_masked_large);
+    int item = blockIdx.x;
+    if (item >= nP + nB + nM) return;
+    const bool chw = fp.to_chw != 0;
+    const bool blur = fp.blur != 0;
+    const float* src = vp.work;
+    float* dst = vp.image;
+    const uint8_t* ltype = fb.large_type + static_cast<size_t>(v) * fp.max_large;
+    const int tid = threadIdx.x;
+    const int W = vp.width, H = vp.height;
+    if (item < nP) {
+        const uint32_t lt = fb.work_low[static_cast<size_t>(v) * fp.max_large + item];
+        const int ltx = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)), lty = static_cast<int>(lt / static_cast<uint32_t>(vp.glw));
+        const int ox = ltx * kTileLarge, oy = lty * kTileLarge;
+        const int n = blur ? 10 : 9;
+        const int bx = blur ? ox - kStride : ox, by = blur ? oy - kStride : oy;
+        const int max_r = static_cast<int>((static_cast<unsigned>(W) - static_cast<unsigned>(bx) - 1u) / static_cast<unsigned>(kStride));
+        const int max_d = static_cast<int>((static_cast<unsigned>(H) - static_cast<unsigned>(by) - 1u) / static_cast<unsigned>(kStride));
+        float3* s = s_samples[0];
+        for (int k = tid; k < n * n; k += 256)
+            s[k] = grid_sample(vp, ltype, src, chw, bx, by, k % n, k / n, max_r, max_d, ltx, lty, blur);
+        __syncthreads();
+        const int lx = tid & 15, ly = tid >> 4;
+        const int px = ox + lx, py = oy + ly;
+        if (px >= W || py >= H) return;
+        if (!blur) {
+            if ((lx % kStride) == 0 && (ly % kStride) == 0) return;
+            const float3 r = bilerp(s, 9, lx, ly);
+            store_rgb(dst, W, H, px, py, chw, __saturatef(r.x), __saturatef(r.y), __saturatef(r.z));
+        } else {
+            float f;
+            const float3 r = blur5(s, 10, lx, ly, f);
+            store_rgb(dst, W, H, px, py, chw, __saturatef(r.x * f), __saturatef(r.y * f), __saturatef(r.z * f));
+        }
+        return;
+    }
+    item -= nP;
+    if (item < nB) {
+        const uint32_t lt = fb.work_full[static_cast<size_t>(v) * fp.max_large + st.n_fovea_large + item];
+        const int ltx = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)), lty = static_cast<int>(lt / static_cast<uint32_t>(vp.glw));
+        const int g = tid >> 6, t = tid & 63;  // sub-tile group
+        const int ox = ltx * kTileLarge + (g % kStride) * kTileSmall, oy = lty * kTileLarge + (g / kStride) * kTileSmall;
+        const int n = blur ? 6 : 5;
+        const int bx = blur ? ox - kStride : ox, by = blur ? oy - kStride : oy;
+        const int max_r = static_cast<int>((static_cast<unsigned>(W) - static_cast<unsigned>(bx) - 1u) / static_cast<unsigned>(kStride));
+        const int max_d = static_cast<int>((static_cast<unsigned>(H) - static_cast<unsigned>(by) - 1u) / static_cast<unsigned>(kStride));
+        float3* s = s_samples[g];
+        for (int k = t; k < n * n; k += 64)
+            s[k] = grid_sample(vp, ltype, src, chw, bx, by, k % n, k / n, max_r, max_d, ltx, lty, blur);
+        __syncthreads();
+        const int lx = t & 7, ly = t >> 3;
+        const int px = ox + lx, py = oy + ly;
+        if (px >= W || py >= H) return;
+        const float2 dg = vp.gaze_px - make_float2(static_cast<float>(px), static_cast<float>(py));
+        const float bf = clampf((length(dg) - kBlendRadiusPx - kTileLarge) / (kBlendWidthPx - kTileLarge), 0.0f, 1.0f);
+        if (!blur) {
+            if ((lx % kStride) == 0 && (ly % kStride) == 0) return;
+            const float3 r = bilerp(s, 5, lx, ly);
+            const float3 cc = load_rgb(src, W, H, px, py, chw);
+            if (bf > 0.0f)
+                store_rgb(dst, W, H, px, py, chw, __saturatef(r.x * bf + cc.x * (1.0f - bf)),
+                          __saturatef(r.y * bf + cc.y * (1.0f - bf)), __saturatef(r.z * bf + cc.z * (1.0f - bf)));
+        } else {
+            float f;
+            const float3 r = blur5(s, 6, lx, ly, f);
+            const float3 cc = load_rgb(src, W, H, px, py, chw);
+            if (bf > 0.0f)
+                store_rgb(dst, W, H, px, py, chw, __saturatef(cc.x * (1.0f - bf) + r.x * f * bf),
+                          __saturatef(cc.y * (1.0f - bf) + r.y * f * bf), __saturatef(cc.z * (1.0f - bf) + r.z * f * bf));
+            else
+                store_rgb(dst, W, H, px, py, chw, cc.x, cc.y, cc.z);
+        }
+        return;
+    }
+    item -= nB;
+    {
+        const uint32_t lt = fb.work_masked[static_cast<size_t>(v) * fp.max_large + item];
+        const int ox = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)) * kTileLarge;
+        const int oy = static_cast<int>(lt / static_cast<uint32_t>(vp.glw)) * kTileLarge;
+        const int px = ox + (tid & 15), py = oy + (tid >> 4);
+        if (px < W && py < H) store_rgb(dst, W, H, px, py, chw, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+int launch_compose(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s) {
+    if (fp.max_large == 0) return 0;
+    compose_kernel<<<dim3(fp.max_large, fp.n_views), 256, 0, s>>>(fp, fb);
+    return 1;
+}
+
+const KernelSet& kernel_set() {
+    static const KernelSet ks = {launch_setup,  launch_classify, launch_preprocess, launch_scan_blocks, launch_create,
+                                 launch_sort,   launch_ranges,   launch_blend,      launch_compose};
+    return ks;
+}
+
+}  // namespace FHTGS_FLAVOR
+}  // namespace fhtgs

@@ -1,0 +1,149 @@
+// Shared host/device definitions of the fhtgs renderer: constants, per-view parameters,
+// frame buffers and the table of kernel launchers each math flavour exports.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fhtgs {
+
+// Renderer constants; identical values to rasterization/include/config.h:13-45 of the
+// reference (thresholds, tile sizes, foveation radius 375 px / blend band 125 px).
+constexpr float kTransmittanceThreshold = 1e-4f;
+constexpr float kMaxFragmentAlpha = 1.0f;
+constexpr float kMinAlphaRcp = 255.0f;
+constexpr float kMinAlpha = 1.0f / kMinAlphaRcp;
+constexpr float kMaxCutoffSq = 11.0825270903f;
+constexpr float kMinAlphaCore = 1.0f / 20.0f;
+constexpr int kTileSmall = 8;
+constexpr int kTileLarge = 16;
+constexpr int kStride = kTileLarge / kTileSmall;      // 2
+constexpr int kSubTiles = kStride * kStride;          // 4
+constexpr int kFoveaRadiusPx = 375;
+constexpr int kFoveaRadiusTiles = (kFoveaRadiusPx + kTileLarge - 1) / kTileLarge;  // 24
+constexpr int kBlendWidthPx = 125;
+constexpr int kBlendRadiusTiles = (kFoveaRadiusPx - kBlendWidthPx) / kTileLarge;   // 15
+constexpr int kBlendRadiusPx = kBlendRadiusTiles * kTileLarge;                     // 240
+constexpr int kFoveaTableSide = 2 * kFoveaRadiusTiles + 1;                         // 49
+
+enum TileType : uint8_t { kFovea = 0, kPeriphery = 1, kBlended = 2, kMasked = 3 };
+
+// Per-view parameters, resident in device memory for the whole frame (filled by the
+// setup kernel from the caller's device matrices and host scalars).
+struct ViewParams {
+    float4 M[3];
+    float4 VPM[4];
+    float4 VPR_inv[4];
+    float4 cam;            // xyz
+    float2 gaze_px;        // clamped to the image (inference.cu:79-82)
+    float2 gaze_tiles;     // float of the int gaze tile (inference.cu:98-105)
+    int2 gaze_tiles_i;
+    int width, height;
+    float focal_x, focal_y, center_x, center_y;
+    int glw, glh;          // large-tile grid
+    int n_large, n_tiles;  // large tiles, small-tile ids (4 per large tile)
+    const uint32_t* vis_mask;
+    const uint32_t* vis_sat;
+    const uint32_t* fovea_sat;
+    float* image;          // final image
+    float* work;           // blend target of periphery/blended tiles (temp buffer when blurring)
+};
+
+// Host-side description of a view before the setup kernel runs.
+struct ViewSetup {
+    const float* M;
+    const float* VPM;
+    const float* VPR_inv;
+    const float* cam;
+    ViewParams p;          // scalars filled on the host, matrices gathered on the device
+};
+
+// Settings shared by all views of a frame (kernel parameter, by value).
+struct FrameParams {
+    int n_views;
+    int n_prims;
+    int total_sh;          // S
+    int active_sh;
+    int K;
+    float near_plane, far_plane, scale_modifier;
+    int to_chw, blur, aaa;
+    int bg_type;
+    const float* bg_data;
+    int tex_w, tex_h;
+    int key_u32;           // 0: 16-bit keys, 1: 32-bit keys
+    int end_bit;           // bits sorted (max over views)
+    int64_t cap;           // instance slots per view
+    int max_tiles;         // max small-tile ids over views (stride of per-tile arrays)
+    int max_large;         // max large tiles over views
+    int n_blocks_prim;     // preprocess/create blocks per view
+};
+
+// Per-view frame status written by the device, read by the host after the frame.
+struct FrameStatus {
+    unsigned long long n_instances;   // M (64-bit sum)
+    uint32_t n_active;                // entries in the partitioned tile map
+    uint32_t ranges[6];               // partition ranges (fovea, periphery, blended)
+    uint32_t n_fovea_large, n_blended_large, n_periphery_large, n_masked_large;
+    uint32_t overflow;
+    uint32_t pad;
+};
+
+struct Gaussians {
+    const float* positions;
+    const float* scales;
+    const float* rotations;
+    const float* opacities;
+    const float* sh_0;
+    const float* sh_rest;
+};
+
+// All per-frame device buffers (arena carve-up); arrays are [view][...] with the strides
+// recorded in FrameParams.
+struct FrameBuffers {
+    ViewParams* views;
+    FrameStatus* status;
+    uint32_t* n_touched;      // [V][N]
+    ushort4* bounds;          // [V][N]
+    float4* rec;              // [V][N][4]: VPMT1, VPMT2, VPMT4, rgba
+    uint32_t* block_sums;     // [V][n_blocks_prim]
+    void* keys[2];            // [V][cap] uint16 or uint32
+    uint32_t* vals[2];        // [V][cap]
+    int final_buf;            // which of keys/vals holds the sorted result
+    uint32_t* sort_hist;      // [V][256][sort_tiles]
+    uint32_t* sort_digit_tot; // [V][256]
+    int sort_tiles;           // tiles of the radix sort per view (capacity based)
+    uint2* ranges;            // [V][max_tiles]
+    uint32_t* tile_map_part;  // [V][max_tiles]
+    uint8_t* tile_type_part;  // [V][max_tiles]
+    uint8_t* large_type;      // [V][max_large]
+    uint32_t* work_full;      // [V][max_large] fovea then blended large tiles
+    uint32_t* work_low;       // [V][max_large] periphery large tiles
+    uint32_t* work_masked;    // [V][max_large] masked large tiles
+    uint32_t* counters;       // [4] persistent-kernel work counters
+};
+
+// Launchers exported by each math flavour (fast = -use_fast_math, ieee = default).
+struct KernelSet {
+    // Each launcher returns the number of kernels it launched.
+    int (*setup)(const ViewSetup* setups, int n_views, ViewParams* out, cudaStream_t s);
+    int (*classify)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);
+    int (*preprocess)(const FrameParams& fp, const FrameBuffers& fb, const Gaussians& g, cudaStream_t s);
+    int (*scan_blocks)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);
+    int (*create_instances)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);
+    int (*sort)(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s);
+    int (*ranges)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);
+    // `mid` (may be null) is recorded between the full-resolution and the periphery blend.
+    int (*blend)(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid);
+    int (*compose)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);
+};
+
+const KernelSet& kernels_fast();
+const KernelSet& kernels_ieee();
+
+constexpr int kPrimBlock = 256;      // preprocess / create-instances block
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;        // keys per thread per sort tile
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
+constexpr int kSortRadixBits = 8;
+constexpr int kSortBins = 1 << kSortRadixBits;
+
+}  // namespace fhtgs

@@ -1,0 +1,217 @@
+/*
+ * fhtgs — B200-native forward renderer for foveated hybrid-transparency Gaussian splatting.
+ *
+ * C ABI of libfhtgs.so.  Plain pointers and sizes only; no torch types.  All pointers marked
+ * "device" must point to CUDA device memory of the context's device; "host" values are read
+ * during the call.  Calls are asynchronous on the given stream unless the name ends in
+ * `_sync`.  A context is not thread-safe: use one context per host thread (contexts may
+ * share a device).
+ *
+ * Reference interfaces replaced (paths relative to the reference's FoveatedHTGSCudaBackend/
+ * package directory):
+ *   fhtgs_render_mono       <- _C.render            = inference_wrapper
+ *                              (rasterization/src/inference_api.cu:13-43, torch_bindings/bindings.cpp:8)
+ *   fhtgs_benchmark_mono    <- _C_benchmarking.benchmark = fast_inference_wrapper
+ *                              (rasterization/src/fast_inference_api.cu:12-43, torch_bindings/bindings_benchmarking.cpp:7)
+ *   fhtgs_render_stereo     <- _C_stereo.render     = inference_stereo_wrapper
+ *                              (rasterization/src/inference_stereo_api.cu:13-67, torch_bindings/bindings_stereo.cpp:8)
+ *   fhtgs_render_views      <- inference() / inference_stereo() generalised to n views
+ *                              (rasterization/src/inference.cu:49-472, inference_stereo.cu:49-828)
+ */
+#ifndef FHTGS_H_
+#define FHTGS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FHTGS_ABI_VERSION 1
+
+typedef enum {
+    FHTGS_OK = 0,
+    FHTGS_ERR_INVALID_ARGUMENT = 1, /* bad shape, null pointer, unsupported option       */
+    FHTGS_ERR_CUDA = 2,             /* a CUDA runtime call failed (see fhtgs_last_error) */
+    FHTGS_ERR_OUT_OF_MEMORY = 3,    /* device arena could not grow                        */
+    FHTGS_ERR_CAPACITY = 4,         /* instance count exceeded the arena; re-run (the
+                                       _sync entry points grow and retry by themselves)   */
+    FHTGS_ERR_NOT_READY = 5         /* no completed frame to inspect                      */
+} fhtgs_status;
+
+/* Background models, as the reference's BackgroundModelType (rasterization_utils.h:6-11). */
+typedef enum {
+    FHTGS_BACKGROUND_NONE = 0,
+    FHTGS_BACKGROUND_SH = 1,          /* data: device float[16*3]                           */
+    FHTGS_BACKGROUND_TEXTURE = 2,     /* data: device float[3*h*w], equirectangular         */
+    FHTGS_BACKGROUND_TEXTURE_RAW = 3  /* as TEXTURE, sigmoid applied after interpolation   */
+} fhtgs_background_type;
+
+typedef struct fhtgs_context_s* fhtgs_context;
+
+/* Gaussians (device, float32, contiguous, activated parameters). */
+typedef struct {
+    const float* positions;  /* [N,3]                                   */
+    const float* scales;     /* [N,3] linear                            */
+    const float* rotations;  /* [N,4] (w,x,y,z), used as given          */
+    const float* opacities;  /* [N] post-sigmoid                        */
+    const float* sh_0;       /* [N,3]                                   */
+    const float* sh_rest;    /* [N,S,3], may be NULL when S == 0        */
+    int32_t n_primitives;    /* N                                       */
+    int32_t total_sh_bases;  /* S = sh_rest.size(1)                     */
+} fhtgs_primitives;
+
+/* One camera and its output image. */
+typedef struct {
+    const float* M;        /* device [3,4] world -> view                       */
+    const float* VPM;      /* device [4,4] world -> screen                     */
+    const float* VPR_inv;  /* device [4,4] screen -> world direction           */
+    const float* cam_position;   /* device [3]                                 */
+    float gaze_x, gaze_y;        /* host: gaze in pixels                       */
+    const uint32_t* visibility_mask;            /* device, 1 bit per 16x16 tile   */
+    const uint32_t* visibility_mask_area_table; /* device, (gx+1)*(gy+1)          */
+    const uint32_t* fovea_mask_area_table;      /* device, 49*49                  */
+    int32_t width, height;
+    float focal_x, focal_y, center_x, center_y;
+    float* image;          /* device output, [3,H,W] (to_chw) or [H,W,3]         */
+} fhtgs_view;
+
+typedef struct {
+    int32_t K;                 /* core size; rounded down to a power of two <= 32   */
+    int32_t active_sh_bases;   /* 1, 4, 9 or 16                                     */
+    float near_plane, far_plane, scale_modifier;
+    int32_t to_chw, blur_periphery, anti_aliasing;
+    int32_t background_type;   /* fhtgs_background_type                             */
+    const float* background_data;
+    int32_t texture_width, texture_height;
+    int32_t fast_math;         /* 1: arithmetic of _C_benchmarking/_C_stereo
+                                  (-use_fast_math); 0: IEEE arithmetic of _C         */
+} fhtgs_settings;
+
+/* Per-view facts of the last frame rendered by a context (read after it completed). */
+typedef struct {
+    int64_t n_instances;       /* M = sum of touched tiles (includes sentinel slots) */
+    int64_t instance_capacity; /* arena slots available per view                     */
+    uint32_t n_active_tiles;   /* small-tile entries in the tile index map           */
+    uint32_t partition_ranges[6]; /* fovea, periphery, blended [begin,end)           */
+    int32_t overflow;          /* 1 when n_instances > instance_capacity             */
+    int32_t end_bit;           /* key bits sorted                                   */
+} fhtgs_frame_info;
+
+/* Intermediates of one view of the last frame, copied to HOST buffers (any may be NULL).
+ * Keys are widened to uint32; sentinels are 0xFFFF (16-bit keys) or 0xFFFFFFFF. */
+typedef struct {
+    uint32_t* n_touched;      /* [N]           */
+    uint16_t* screen_bounds;  /* [N,4]         */
+    float* vpmt;              /* [N,12] VPMT1, VPMT2, VPMT4 */
+    float* rgba;              /* [N,4]         */
+    uint32_t* tile_index_map_partitioned; /* [n_active_tiles] */
+    uint8_t* tile_type_partitioned;       /* [n_active_tiles] */
+    uint32_t* keys;           /* [n_instances] sorted */
+    uint32_t* values;         /* [n_instances] sorted */
+    uint32_t* instance_ranges;/* [2*T], T = 4 * ceil(W/16) * ceil(H/16) */
+} fhtgs_intermediates;
+
+/* ---- context ---- */
+fhtgs_status fhtgs_context_create(int32_t device, fhtgs_context* out);
+fhtgs_status fhtgs_context_destroy(fhtgs_context ctx);
+/* Reserve arena space for up to n_views views of n_primitives Gaussians with the given
+ * instance capacity per view (0: estimate).  Optional; rendering grows the arena. */
+fhtgs_status fhtgs_context_reserve(fhtgs_context ctx, int32_t n_primitives, int32_t n_views,
+                                   int32_t max_width, int32_t max_height, int64_t instances_per_view);
+size_t fhtgs_context_arena_bytes(fhtgs_context ctx);
+/* Total kernels this context has launched (all frames). */
+int64_t fhtgs_context_launch_count(fhtgs_context ctx);
+
+/* ---- stage timing ----
+ * With profiling on, every frame records CUDA events on its stream between the stages:
+ *   0 setup+classify, 1 preprocess, 2 scan+create instances, 3 sort, 4 tile ranges,
+ *   5 blend full-resolution tiles, 6 blend periphery tiles, 7 compose.
+ * fhtgs_get_stage_times waits for the last frame and returns the milliseconds per stage. */
+#define FHTGS_N_STAGES 8
+fhtgs_status fhtgs_context_set_profiling(fhtgs_context ctx, int32_t enable);
+fhtgs_status fhtgs_get_stage_times(fhtgs_context ctx, float* ms, int32_t n);
+/* Stage times of up to the last 64 profiled frames, oldest first: ms[f*FHTGS_N_STAGES + s]. */
+fhtgs_status fhtgs_get_stage_history(fhtgs_context ctx, float* ms, int32_t max_frames, int32_t* n_frames);
+
+/* ---- rendering ---- */
+/* Renders n_views views of one scene, asynchronously on `stream` (cudaStream_t).
+ * Returns FHTGS_OK once queued; instance overflow is reported by fhtgs_get_frame_info after the
+ * stream has completed the frame. */
+fhtgs_status fhtgs_render_views(fhtgs_context ctx, const fhtgs_primitives* prims,
+                                const fhtgs_view* views, int32_t n_views,
+                                const fhtgs_settings* settings, void* stream);
+/* As fhtgs_render_views, then waits for the frame; on instance overflow it grows the arena
+ * and renders again, so the images are always complete on FHTGS_OK. */
+fhtgs_status fhtgs_render_views_sync(fhtgs_context ctx, const fhtgs_primitives* prims,
+                                     const fhtgs_view* views, int32_t n_views,
+                                     const fhtgs_settings* settings, void* stream);
+fhtgs_status fhtgs_get_frame_info(fhtgs_context ctx, int32_t view, fhtgs_frame_info* out);
+fhtgs_status fhtgs_copy_intermediates(fhtgs_context ctx, int32_t view, fhtgs_intermediates* out);
+
+/* ---- drop-in mirrors of the reference's positional entry points (blocking) ----
+ * Arguments follow the reference's order; tensors become device pointers (+ the sizes the
+ * reference reads from tensor shapes), gaze_position becomes two host floats, and the output
+ * image(s) are caller-allocated device buffers. */
+fhtgs_status fhtgs_render_mono(
+    fhtgs_context ctx,
+    const float* positions, const float* scales, const float* rotations, const float* opacities,
+    const float* sh_0, const float* sh_rest, int32_t n_primitives, int32_t total_sh_bases,
+    const float* M, const float* VPM, const float* VPR_inv, const float* cam_position,
+    float gaze_x, float gaze_y,
+    const uint32_t* visibility_mask, const uint32_t* visibility_mask_area_table,
+    const uint32_t* fovea_mask_area_table,
+    const float* background_model_data, int32_t texture_width, int32_t texture_height,
+    int32_t background_model_type, int32_t K, int32_t active_sh_bases, int32_t width, int32_t height,
+    float focal_x, float focal_y, float center_x, float center_y,
+    float near_plane, float far_plane, float scale_modifier,
+    int32_t to_chw, int32_t blur_periphery, int32_t anti_aliasing,
+    float* image, void* stream);
+/* Same arguments; the fast-math arithmetic of the reference's benchmarking module. */
+fhtgs_status fhtgs_benchmark_mono(
+    fhtgs_context ctx,
+    const float* positions, const float* scales, const float* rotations, const float* opacities,
+    const float* sh_0, const float* sh_rest, int32_t n_primitives, int32_t total_sh_bases,
+    const float* M, const float* VPM, const float* VPR_inv, const float* cam_position,
+    float gaze_x, float gaze_y,
+    const uint32_t* visibility_mask, const uint32_t* visibility_mask_area_table,
+    const uint32_t* fovea_mask_area_table,
+    const float* background_model_data, int32_t texture_width, int32_t texture_height,
+    int32_t background_model_type, int32_t K, int32_t active_sh_bases, int32_t width, int32_t height,
+    float focal_x, float focal_y, float center_x, float center_y,
+    float near_plane, float far_plane, float scale_modifier,
+    int32_t to_chw, int32_t blur_periphery, int32_t anti_aliasing,
+    float* image, void* stream);
+/* Stereo: as the reference, K, SH bases, near/far, scale modifier and background model of
+ * the LEFT settings apply to both eyes (inference_stereo_api.cu:111-120,180-186). */
+fhtgs_status fhtgs_render_stereo(
+    fhtgs_context ctx,
+    const float* positions, const float* scales, const float* rotations, const float* opacities,
+    const float* sh_0, const float* sh_rest, int32_t n_primitives, int32_t total_sh_bases,
+    const float* M_left, const float* VPM_left, const float* VPR_inv_left, const float* cam_position_left,
+    float gaze_x_left, float gaze_y_left,
+    const uint32_t* visibility_mask_left, const uint32_t* visibility_mask_area_table_left,
+    const uint32_t* fovea_mask_area_table_left,
+    const float* background_model_data_left, int32_t texture_width_left, int32_t texture_height_left,
+    int32_t background_model_type_left, int32_t K_left, int32_t active_sh_bases_left,
+    int32_t width_left, int32_t height_left,
+    float focal_x_left, float focal_y_left, float center_x_left, float center_y_left,
+    float near_plane_left, float far_plane_left, float scale_modifier_left,
+    const float* M_right, const float* VPM_right, const float* VPR_inv_right, const float* cam_position_right,
+    float gaze_x_right, float gaze_y_right,
+    const uint32_t* visibility_mask_right, const uint32_t* visibility_mask_area_table_right,
+    const uint32_t* fovea_mask_area_table_right,
+    int32_t width_right, int32_t height_right,
+    float focal_x_right, float focal_y_right, float center_x_right, float center_y_right,
+    int32_t to_chw, int32_t blur_periphery, int32_t anti_aliasing,
+    float* image_left, float* image_right, void* stream);
+
+/* ---- errors / version ---- */
+const char* fhtgs_last_error(void);   /* thread-local message of the last failure */
+int32_t fhtgs_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FHTGS_H_ */
