@@ -197,14 +197,24 @@ int launch_classify(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t 
 // ------------------------------------------------------------------------------------------
 struct Mat3 { float r11, r12, r13, r21, r22, r23, r31, r32, r33; };
 
+// Quaternion (w,x,y,z), not normalised, to rotation matrix (kernel_utils.cuh:76-88 of the
+// reference).  Which product of each sum is fused into an FMA decides the last bit of the
+// result; the choice below is the one the reference's build makes (established from its
+// outputs: tests/golden and the live comparison), written with explicit intrinsics so that
+// it no longer depends on the compiler's contraction heuristics.
 __device__ __forceinline__ Mat3 quat_to_rot(const float4 q) {
     const float r = q.x, x = q.y, y = q.z, z = q.w;
-    const float xx = x * x, yy = y * y, zz = z * z;
-    const float xy = x * y, xz = x * z, yz = y * z;
-    const float rx = r * x, ry = r * y, rz = r * z;
-    return {1.0f - 2.0f * (yy + zz), 2.0f * (xy - rz), 2.0f * (xz + ry),
-            2.0f * (xy + rz), 1.0f - 2.0f * (xx + zz), 2.0f * (yz - rx),
-            2.0f * (xz - ry), 2.0f * (yz + rx), 1.0f - 2.0f * (xx + yy)};
+    const float xx = __fmul_rn(x, x), yy = __fmul_rn(y, y), zz = __fmul_rn(z, z);
+    const float xy = __fmul_rn(x, y), xz = __fmul_rn(x, z), yz = __fmul_rn(y, z);
+    const float rx = __fmul_rn(r, x), ry = __fmul_rn(r, y), rz = __fmul_rn(r, z);
+    return {__fmaf_rn(-2.0f, __fadd_rn(yy, zz), 1.0f), 2.0f * __fmaf_rn(x, y, -rz), 2.0f * __fmaf_rn(r, y, xz),
+            2.0f * __fmaf_rn(x, y, rz), __fmaf_rn(-2.0f, __fmaf_rn(x, x, zz), 1.0f), 2.0f * __fmaf_rn(y, z, -rx),
+            2.0f * __fmaf_rn(-r, y, xz), 2.0f * __fmaf_rn(y, z, rx), __fmaf_rn(-2.0f, __fmaf_rn(x, x, yy), 1.0f)};
+}
+
+// n . a with the left-to-right fused evaluation ((n.x a.x) + n.y a.y) + n.z a.z.
+__device__ __forceinline__ float dot3_lr(const float3 n, const float3 a) {
+    return __fmaf_rn(n.z, a.z, __fmaf_rn(n.y, a.y, __fmul_rn(n.x, a.x)));
 }
 
 // Real spherical-harmonics basis constants (degree <= 3).
@@ -256,7 +266,12 @@ __device__ __forceinline__ uint32_t touched_from_bounds(const ViewParams& vp, co
 
 __device__ __forceinline__ float4 xform_row(const float4 P, float3 u, float3 v, float3 w, float3 pos) {
     const float3 n = xyz(P);
-    return make_float4(dot(n, u), dot(n, v), dot(n, w), dot(n, pos) + P.w);
+    return make_float4(dot3_lr(n, u), dot3_lr(n, v), dot3_lr(n, w), __fadd_rn(dot3_lr(n, pos), P.w));
+}
+
+// Column c of R scaled by s then by the scale modifier: ((R_ic * s) * m).
+__device__ __forceinline__ float3 scaled_axis(float a, float b, float c, float s, float m) {
+    return make_float3(__fmul_rn(__fmul_rn(a, s), m), __fmul_rn(__fmul_rn(b, s), m), __fmul_rn(__fmul_rn(c, s), m));
 }
 
 // Standard (non anti-aliased) transform and cull.  Returns true when culled.
@@ -267,9 +282,9 @@ __device__ __forceinline__ bool transform_and_cull(const ViewParams& vp, const F
     const float z = dot(xyz(M3), pos) + M3.w;
     if (z < fp.near_plane || z > fp.far_plane) return true;
     const Mat3 R = quat_to_rot(quat);
-    const float3 u = make_float3(R.r11 * scale.x, R.r21 * scale.x, R.r31 * scale.x) * fp.scale_modifier;
-    const float3 v = make_float3(R.r12 * scale.y, R.r22 * scale.y, R.r32 * scale.y) * fp.scale_modifier;
-    const float3 w = make_float3(R.r13 * scale.z, R.r23 * scale.z, R.r33 * scale.z) * fp.scale_modifier;
+    const float3 u = scaled_axis(R.r11, R.r21, R.r31, scale.x, fp.scale_modifier);
+    const float3 v = scaled_axis(R.r12, R.r22, R.r32, scale.y, fp.scale_modifier);
+    const float3 w = scaled_axis(R.r13, R.r23, R.r33, scale.z, fp.scale_modifier);
     P4 = xform_row(vp.VPM[3], u, v, w, pos);
     const float rho_cutoff = 2.0f * logf(opacity * kMinAlphaRcp);
     const float4 d = make_float4(rho_cutoff, rho_cutoff, rho_cutoff, -1.0f);
@@ -410,9 +425,9 @@ __device__ __forceinline__ bool transform_and_cull_aaa(const ViewParams& vp, con
     const float3 cg = make_float3(R.r11 * cs.x + R.r21 * cs.y + R.r31 * cs.z, R.r12 * cs.x + R.r22 * cs.y + R.r32 * cs.z,
                                   R.r13 * cs.x + R.r23 * cs.y + R.r33 * cs.z) / sc;
     if (dot(cg, cg) < rho_cutoff) return true;
-    const float3 u = make_float3(R.r11 * sc.x, R.r21 * sc.x, R.r31 * sc.x) * fp.scale_modifier;
-    const float3 v = make_float3(R.r12 * sc.y, R.r22 * sc.y, R.r32 * sc.y) * fp.scale_modifier;
-    const float3 w = make_float3(R.r13 * sc.z, R.r23 * sc.z, R.r33 * sc.z) * fp.scale_modifier;
+    const float3 u = scaled_axis(R.r11, R.r21, R.r31, sc.x, fp.scale_modifier);
+    const float3 v = scaled_axis(R.r12, R.r22, R.r32, sc.y, fp.scale_modifier);
+    const float3 w = scaled_axis(R.r13, R.r23, R.r33, sc.z, fp.scale_modifier);
     P1 = xform_row(vp.VPM[0], u, v, w, pos);
     P2 = xform_row(vp.VPM[1], u, v, w, pos);
     const float4 P3 = xform_row(vp.VPM[2], u, v, w, pos);
@@ -947,9 +962,12 @@ __global__ void __launch_bounds__(LOWRES ? 64 : 256) blend_kernel(FrameParams fp
     __shared__ float4 s_p1[NT], s_p2[NT], s_p4[NT], s_rgba[NT];
     __shared__ uint32_t s_mask[NT];
     __shared__ int s_item;
+    // Warp w covers 8 x 4 samples: full resolution lays the 8 warps out 2 x 4 over the 16 x 16
+    // tile, the periphery grid (8 x 8 samples at stride 2) stacks its 2 warps vertically.
+    constexpr int WX = LOWRES ? 1 : 2;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int lx = (warp & 1) * 8 + (lane & 7);
-    const int ly = (warp >> 1) * 4 + (lane >> 3);
+    const int lx = (warp % WX) * 8 + (lane & 7);
+    const int ly = (warp / WX) * 4 + (lane >> 3);
     // total work items over all views
     int total = 0;
     for (int v = 0; v < fp.n_views; ++v) {
@@ -980,9 +998,6 @@ __global__ void __launch_bounds__(LOWRES ? 64 : 256) blend_kernel(FrameParams fp
         const bool inside = px_i < vp.width && py_i < vp.height;
         const float pixel_x = __uint2float_rn(static_cast<uint32_t>(px_i));
         const float pixel_y = __uint2float_rn(static_cast<uint32_t>(py_i));
-        // warp rectangle in pixels
-        const float wx0 = static_cast<float>(ox + (warp & 1) * 8 * S), wx1 = wx0 + 7.0f * S;
-        const float wy0 = static_cast<float>(oy + (warp >> 1) * 4 * S), wy1 = wy0 + 3.0f * S;
         const uint2 range = fb.ranges[static_cast<size_t>(v) * fp.max_tiles + lt * kSubTiles];
         const uint32_t* vals = fb.vals[fb.final_buf] + static_cast<size_t>(v) * fp.cap;
         const float4* rec = fb.rec + 4 * static_cast<size_t>(v) * fp.n_prims;
@@ -1013,8 +1028,8 @@ __global__ void __launch_bounds__(LOWRES ? 64 : 256) blend_kernel(FrameParams fp
                         m = 0u;
 #pragma unroll
                         for (int w = 0; w < NW; ++w) {
-                            const float ax0 = static_cast<float>(ox + (w & 1) * 8 * S), ax1 = ax0 + 7.0f * S;
-                            const float ay0 = static_cast<float>(oy + (w >> 1) * 4 * S), ay1 = ay0 + 3.0f * S;
+                            const float ax0 = static_cast<float>(ox + (w % WX) * 8 * S), ax1 = ax0 + 7.0f * S;
+                            const float ay0 = static_cast<float>(oy + (w / WX) * 4 * S), ay1 = ay0 + 3.0f * S;
                             if (box.y >= ax0 && box.x <= ax1 && box.w >= ay0 && box.z <= ay1) m |= 1u << w;
                         }
                     }
@@ -1022,7 +1037,6 @@ __global__ void __launch_bounds__(LOWRES ? 64 : 256) blend_kernel(FrameParams fp
                 s_mask[tid] = m;
             }
             __syncthreads();
-            (void)wx0; (void)wx1; (void)wy0; (void)wy1;
             for (uint32_t j = 0; j < n_batch; ++j) {
                 if (!((s_mask[j] >> warp) & 1u)) continue;
                 if (!inside) continue;

@@ -118,11 +118,11 @@ def _texture_size(bg_type: int, data: torch.Tensor) -> tuple[int, int]:
 
 
 def _check_gaussians(positions, scales, rotations, opacities, sh_0, sh_rest):
-    n = positions.shape[0]
     if positions.dim() != 2 or positions.shape[1] != 3:
         raise ValueError("positions must be [N,3]")
+    n = positions.shape[0]
     for name, t, w in (("scales", scales, 3), ("rotations", rotations, 4)):
-        if t.shape[0] != n or t.reshape(n, -1).shape[1] != w:
+        if t.shape[0] != n or t.numel() != n * w:
             raise ValueError(f"{name} must be [N,{w}]")
     if opacities.numel() != n:
         raise ValueError("opacities must hold N values")

@@ -22,8 +22,8 @@ def settings_from_view(v: _scene.View, *, K: int = 8, active_sh_bases: int = 16,
     def f(a):
         return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(device)
 
-    def u(a):
-        return torch.from_numpy(np.ascontiguousarray(a, np.uint32).view(np.int32)).to(device)
+    def u(a):  # torch.uint32: the reference's bindings read these with data_ptr<uint>()
+        return torch.from_numpy(np.ascontiguousarray(a, np.uint32)).to(device)
 
     bg = np.zeros((1,), np.float32) if background_data is None else background_data
     return RasterizerSettings(

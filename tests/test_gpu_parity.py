@@ -124,12 +124,26 @@ def test_live_reference_intermediates_and_images(renderer, ci):
         assert_instances_equal(inter[i], ref, ref["end_bit"], what)
     mod = REF.module(c["module"])
     args = (c["to_chw"], c["blur"], c["aaa"])
-    if c["module"] == "_C_stereo":
-        refs = mod.render(*gt, *st[0].as_tuple(), *st[1].as_tuple(), *args)
-    else:
-        refs = ((mod.render if c["module"] == "_C" else mod.benchmark)(*gt, *st[0].as_tuple(), *args),)
-    for i, r in enumerate(refs):
-        assert_image_close(imgs[i], r.cpu().numpy(), f"live{ci}/view{i}")
+
+    def ref_images():
+        if c["module"] == "_C_stereo":
+            out = mod.render(*gt, *st[0].as_tuple(), *st[1].as_tuple(), *args)
+        else:
+            out = ((mod.render if c["module"] == "_C" else mod.benchmark)(*gt, *st[0].as_tuple(), *args),)
+        torch.cuda.synchronize()
+        return [o.cpu().numpy() for o in out]
+
+    first, second = ref_images(), ref_images()
+    for i in range(len(views)):
+        if np.array_equal(first[i], second[i]):
+            assert_image_close(imgs[i], first[i], f"live{ci}/view{i}")
+        else:
+            # The reference does not reproduce itself on this input (observed for the left eye
+            # of _C_stereo: fovea tiles left unwritten); the oracle is the judge here.
+            kw = dict(K=c["K"], active_sh_bases=c["active_sh"], to_chw=c["to_chw"], blur=c["blur"], aaa=c["aaa"],
+                      background=bg, background_type=c["background"], precision=32)
+            p = psnr(imgs[i], O.render(g, views[i], **kw))
+            assert p >= 80.0, f"live{ci}/view{i}: reference not reproducible; PSNR vs oracle {p:.1f} dB"
 
 
 @needs_ref

@@ -7,16 +7,17 @@ inputs; see tests/golden/make_golden.py.  Stage by stage:
     counts and bounds: exact (keys, values, ranges, unsorted emission order);
   * preprocess: touched-tile counts and bounds exact except where a bound lies within float
     rounding of a tile edge (the reference's GPU arithmetic cannot be replayed on the host);
-  * blend + composition fed with the reference's intermediates: PSNR >= 50 dB;
-  * end to end in FP64: PSNR >= 40 dB (RGBA8 quantisation of the K-buffer core flips by one
-    level where FP32 and FP64 straddle a rounding boundary).
+  * blend + composition fed with the reference's intermediates: PSNR >= 80 dB (measured
+    90-94 dB on the committed fixtures);
+  * end to end in FP64: PSNR >= 85 dB (measured 95-100 dB); single pixels can still differ by
+    one RGBA8 level of the K-buffer core where FP32 and FP64 straddle a rounding boundary.
 """
 import numpy as np
 import pytest
 
 import oracle as O
 from golden.make_golden import case_inputs
-from helpers import REF_PSNR_DB, assert_instances_equal, assert_tiles_equal, golden_cases, load_golden, psnr, sentinel_for, view_data
+from helpers import assert_instances_equal, assert_tiles_equal, golden_cases, load_golden, psnr, sentinel_for, view_data
 
 CASES = golden_cases()
 if not CASES:
@@ -79,7 +80,7 @@ def test_blend_compose_from_reference_intermediates(name):
         img = O.blend_compose(v, g.n, ref["vpmt"], ref["rgba"], ref["tile_index_map_partitioned"],
                               ref["partition_ranges"], ref["values"], ref["instance_ranges"], **settings_kw(c, bg, 32))
         p = psnr(img, ref["image"])
-        assert p >= REF_PSNR_DB, f"{name}/view{i}: PSNR {p:.1f} dB"
+        assert p >= 80.0, f"{name}/view{i}: PSNR {p:.1f} dB"
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -89,4 +90,4 @@ def test_end_to_end_fp64(name):
     for i, v in enumerate(views):
         img = O.render(g, v, **settings_kw(c, bg, 64))
         p = psnr(img, data[f"v{i}_image"])
-        assert p >= 40.0, f"{name}/view{i}: PSNR vs reference {p:.1f} dB"
+        assert p >= 85.0, f"{name}/view{i}: PSNR vs reference {p:.1f} dB"
