@@ -57,6 +57,7 @@ def parse(argv=None):
     ap.add_argument("--K", type=int, default=8)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--cpu-budget-s", type=float, default=30.0, help="upper bound of the CPU baseline sample")
     return ap.parse_args(argv)
 
@@ -245,7 +246,8 @@ def run_ours(a, world, rank, local):
     achieved = pairs * FLOP_PER_PAIR / (blend_ms / 1000.0) / 1e12
 
     # ---- e2e through the public drop-in call with host buffers ----
-    e2e_steps = a.e2e_steps or max(3, min(a.steps, 10))
+    e2e = None
+    e2e_steps = 0 if a.no_e2e else (a.e2e_steps or max(3, min(a.steps, 10)))
     host_in = []
     for s in st:
         host_in.append({k: getattr(s, k).detach().cpu().pin_memory() for k in ("M", "VPM", "VPR_inv", "cam_position",
@@ -264,18 +266,21 @@ def run_ours(a, world, rank, local):
         out_host[1].copy_(b_img, non_blocking=True)
         torch.cuda.current_stream(dev).synchronize()
 
-    for _ in range(2):
-        e2e_step()
-    barrier(world)
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
-    e2e_value = world * e2e_steps / (e2e_ms / 1000.0)
+    if e2e_steps > 0:
+        for _ in range(2):
+            e2e_step()
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        e2e = {"value": round(world * e2e_steps / (e2e_ms / 1000.0), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "api": "foveatedhtgscudabackend_b200._C_stereo.render",
+               "steps": e2e_steps}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -294,8 +299,7 @@ def run_ours(a, world, rank, local):
                    "math": "fast (matches _C_stereo)", "l2": "inputs larger than L2 (236 MB scene, 2 x 55 MB images)",
                    "parallelism": f"replicated scene, {world} rank(s) x 1 stereo stream"},
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4), "p99": round(float(np.percentile(lat, 99)), 4)},
-        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "api": "foveatedhtgscudabackend_b200._C_stereo.render"},
+        "e2e": e2e,
         "roofline": {"bound": "fp32", "kernel": "blend_kernel<8,false> (fovea + blended tiles)",
                      "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
                      "frac": round(achieved / peak_fp32, 4), "traffic": None,
