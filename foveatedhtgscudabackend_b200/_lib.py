@@ -96,6 +96,7 @@ SIGNATURES = {
     "fhtgs_render_mono": (_MONO_ARGS, c_i32),
     "fhtgs_benchmark_mono": (_MONO_ARGS, c_i32),
     "fhtgs_render_stereo": (_STEREO_ARGS, c_i32),
+    "fhtgs_sort_instances_noalloc": ([vp, vp, vp, vp, C.c_int64, c_i32, c_i32, vp], c_i32),
 }
 
 _lock = threading.Lock()

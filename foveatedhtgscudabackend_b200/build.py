@@ -31,6 +31,7 @@ UNITS = [
     ("kernels_fast.cu", ["-use_fast_math"]),
     ("kernels_ieee.cu", []),
     ("fhtgs_host.cu", []),
+    ("fhtgs_noalloc.cu", []),
 ]
 HEADERS = ["fhtgs_types.cuh", "fhtgs_math.cuh", "fhtgs_kernels.cuh"]
 

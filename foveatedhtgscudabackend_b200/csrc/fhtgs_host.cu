@@ -63,6 +63,11 @@ ViewGeom geometry(const fhtgs_view& v) {
 
 }  // namespace
 
+namespace fhtgs {
+// Lets other translation units of the library report through fhtgs_last_error().
+void set_last_error(const std::string& msg) { g_error = msg; }
+}  // namespace fhtgs
+
 // Stage boundaries recorded when profiling: start | setup+classify | preprocess |
 // scan+create | sort | ranges | blend full-res | blend periphery | compose.
 constexpr int kStageEvents = 9;

@@ -207,6 +207,24 @@ fhtgs_status fhtgs_render_stereo(
     int32_t to_chw, int32_t blur_periphery, int32_t anti_aliasing,
     float* image_left, float* image_right, void* stream);
 
+/* ---- sorting without device allocation ----
+ * No counterpart in the reference.  For callers that must not allocate device memory — a VR
+ * compositor or display thread that cannot afford the stall of a cudaMalloc/cudaFree, or a
+ * plugin whose host application owns the whole device-memory budget — this runs the
+ * renderer's stable instance sort (tile key, primitive index) with working memory in a fixed
+ * device array inside libfhtgs.so (about 8.3 MB, held by every GPU that loads the library
+ * until the process exits) instead of the context arena.
+ *   keys_in/values_in -> keys_out/values_out: n pairs on the current device, keys of key_bytes
+ *   (2 or 4) bytes sorted stably by their low end_bit bits; inputs are not modified.
+ *   n <= 1048576, larger requests fail with FHTGS_ERR_INVALID_ARGUMENT.
+ * The array is shared by all calls on a device and keeps the last call's contents (nothing in
+ * it needs to start at zero); calls that overlap on the GPU race on it, so serialise them.  The
+ * first call on each device looks up the array's address; make it before any stream capture.
+ * Asynchronous on `stream`; no allocation of any kind. */
+fhtgs_status fhtgs_sort_instances_noalloc(const void* keys_in, const uint32_t* values_in,
+                                          void* keys_out, uint32_t* values_out, int64_t n,
+                                          int32_t key_bytes, int32_t end_bit, void* stream);
+
 /* ---- errors / version ---- */
 const char* fhtgs_last_error(void);   /* thread-local message of the last failure */
 int32_t fhtgs_abi_version(void);
