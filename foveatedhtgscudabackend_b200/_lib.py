@@ -61,7 +61,8 @@ class Settings(C.Structure):
 
 class FrameInfo(C.Structure):
     _fields_ = [("n_instances", C.c_int64), ("instance_capacity", C.c_int64), ("n_active_tiles", C.c_uint32),
-                ("partition_ranges", C.c_uint32 * 6), ("overflow", c_i32), ("end_bit", c_i32)]
+                ("partition_ranges", C.c_uint32 * 6), ("overflow", c_i32), ("end_bit", c_i32),
+                ("n_instances_stored", C.c_int64)]
 
 
 class Intermediates(C.Structure):

@@ -39,7 +39,9 @@ int end_bit_of(uint32_t n) {
 }
 
 struct ViewGeom {
-    int glw, glh, n_large, n_tiles, end_bit;
+    int glw, glh, n_large, n_tiles;
+    int end_bit;       // reference key bits: bit width of (small tiles + 1)
+    int key_bits;      // stored key bits: bit width of the largest large-tile index
     int gaze_tx, gaze_ty;
     float gaze_px, gaze_py;
 };
@@ -53,6 +55,7 @@ ViewGeom geometry(const fhtgs_view& v) {
     g.n_large = g.glw * g.glh;
     g.n_tiles = g.n_large * kSubTiles;
     g.end_bit = end_bit_of(static_cast<uint32_t>(g.n_tiles + 1));
+    g.key_bits = std::max(1, end_bit_of(static_cast<uint32_t>(g.n_large - 1)));
     g.gaze_px = std::min(std::max(v.gaze_x, 0.0f), static_cast<float>(v.width - 1));
     g.gaze_py = std::min(std::max(v.gaze_y, 0.0f), static_cast<float>(v.height - 1));
     const int gw = g.glw * kStride, gh = g.glh * kStride;
@@ -99,8 +102,9 @@ namespace {
 
 struct Layout {
     size_t total = 0;
-    size_t off_views, off_status, off_nt, off_bounds, off_rec, off_bsums, off_keys0, off_keys1, off_vals0, off_vals1;
+    size_t off_views, off_status, off_nt, off_nvis, off_bounds, off_rec, off_bsums, off_keys0, off_keys1, off_vals0, off_vals1;
     size_t off_hist, off_dtot, off_ranges, off_map, off_type, off_ltype, off_wf, off_wl, off_wm, off_ctr, off_temp;
+    size_t off_order0, off_order1;
     std::vector<size_t> temp_offsets;
 };
 
@@ -112,6 +116,7 @@ Layout plan(int V, int64_t N, int nbp, int64_t cap, int key_bytes, int sort_tile
     L.off_views = take(sizeof(ViewParams) * V);
     L.off_status = take(sizeof(FrameStatus) * V);
     L.off_nt = take(4ull * V * N);
+    L.off_nvis = take(4ull * V * N);
     L.off_bounds = take(8ull * V * N);
     L.off_rec = take(64ull * V * N);
     L.off_bsums = take(4ull * V * nbp);
@@ -121,14 +126,16 @@ Layout plan(int V, int64_t N, int nbp, int64_t cap, int key_bytes, int sort_tile
     L.off_vals1 = take(4ull * V * cap);
     L.off_hist = take(4ull * V * kSortBins * sort_tiles);
     L.off_dtot = take(4ull * V * kSortBins);
-    L.off_ranges = take(8ull * V * max_tiles);
+    L.off_ranges = take(8ull * V * max_large);
     L.off_map = take(4ull * V * max_tiles);
     L.off_type = take(1ull * V * max_tiles);
     L.off_ltype = take(1ull * V * max_large);
     L.off_wf = take(4ull * V * max_large);
     L.off_wl = take(4ull * V * max_large);
     L.off_wm = take(4ull * V * max_large);
-    L.off_ctr = take(16);
+    L.off_ctr = take(4ull * kCounterWords);
+    L.off_order0 = take(4ull * V * max_large);
+    L.off_order1 = take(4ull * V * max_large);
     for (int64_t f : temp_floats) L.temp_offsets.push_back(f > 0 ? take(4ull * f) : 0);
     L.total = o;
     return L;
@@ -156,7 +163,7 @@ fhtgs_status ensure_arena(fhtgs_context ctx, size_t bytes) {
 
 fhtgs_status validate(const fhtgs_primitives* p, const fhtgs_view* views, int n_views, const fhtgs_settings* s) {
     if (!p || !views || !s) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
-    if (n_views <= 0) return fail(FHTGS_ERR_INVALID_ARGUMENT, "n_views must be positive");
+    if (n_views <= 0 || n_views > 255) return fail(FHTGS_ERR_INVALID_ARGUMENT, "n_views must be in [1, 255]");
     if (p->n_primitives < 0) return fail(FHTGS_ERR_INVALID_ARGUMENT, "n_primitives must be >= 0");
     if (p->total_sh_bases < 0) return fail(FHTGS_ERR_INVALID_ARGUMENT, "total_sh_bases must be >= 0");
     if (p->n_primitives > 0 && (!p->positions || !p->scales || !p->rotations || !p->opacities || !p->sh_0))
@@ -203,11 +210,11 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
         geo[i] = geometry(views[i]);
         max_tiles = std::max(max_tiles, geo[i].n_tiles);
         max_large = std::max(max_large, geo[i].n_large);
-        end_bit = std::max(end_bit, geo[i].end_bit);
+        end_bit = std::max(end_bit, geo[i].key_bits);
     }
     if (ctx->cap <= 0) ctx->cap = estimate_capacity(N);
     const int64_t cap = ctx->cap;
-    const int key_u32 = end_bit > 16 ? 1 : 0;
+    const int key_u32 = max_large > 65536 ? 1 : 0;
     const int nbp = static_cast<int>((N + kPrimBlock - 1) / kPrimBlock);
     const int sort_tiles = static_cast<int>((cap + kSortTile - 1) / kSortTile);
     std::vector<int64_t> temp_floats(V, 0);
@@ -245,6 +252,7 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     fb.views = reinterpret_cast<ViewParams*>(A + L.off_views);
     fb.status = reinterpret_cast<FrameStatus*>(A + L.off_status);
     fb.n_touched = reinterpret_cast<uint32_t*>(A + L.off_nt);
+    fb.n_vis = reinterpret_cast<uint32_t*>(A + L.off_nvis);
     fb.bounds = reinterpret_cast<ushort4*>(A + L.off_bounds);
     fb.rec = reinterpret_cast<float4*>(A + L.off_rec);
     fb.block_sums = reinterpret_cast<uint32_t*>(A + L.off_bsums);
@@ -264,6 +272,8 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     fb.work_low = reinterpret_cast<uint32_t*>(A + L.off_wl);
     fb.work_masked = reinterpret_cast<uint32_t*>(A + L.off_wm);
     fb.counters = reinterpret_cast<uint32_t*>(A + L.off_ctr);
+    fb.work_order[0] = reinterpret_cast<uint32_t*>(A + L.off_order0);
+    fb.work_order[1] = reinterpret_cast<uint32_t*>(A + L.off_order1);
 
     std::vector<ViewSetup> setups(V);
     for (int i = 0; i < V; ++i) {
@@ -305,7 +315,7 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     };
     long long n = 0;
     mark(0);
-    FHTGS_CK(cudaMemsetAsync(fb.counters, 0, 16, stream));
+    FHTGS_CK(cudaMemsetAsync(fb.counters, 0, 4ull * kCounterWords, stream));
     n += ks.setup(setups.data(), V, fb.views, stream);
     n += ks.classify(fp, fb, stream);
     mark(1);
@@ -318,7 +328,8 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     mark(3);
     n += ks.sort(fp, fb, stream);
     mark(4);
-    n += ks.ranges(fp, fb, stream);
+    n += ks.ranges(fp, fb, ctx->n_sms, stream);
+    n += ks.order(fp, fb, ctx->n_sms, stream);
     mark(5);
     n += ks.blend(fp, fb, ctx->n_sms, stream, prof ? ev[6] : nullptr);
     mark(7);
@@ -480,12 +491,13 @@ fhtgs_status fhtgs_get_frame_info(fhtgs_context ctx, int32_t view, fhtgs_frame_i
     fhtgs_status st = read_status(ctx);
     if (st != FHTGS_OK) return st;
     const FrameStatus& s = ctx->h_status[view];
-    out->n_instances = static_cast<int64_t>(s.n_instances);
+    out->n_instances = static_cast<int64_t>(s.n_instances_ref);
     out->instance_capacity = ctx->fp.cap;
     out->n_active_tiles = s.n_active;
     for (int k = 0; k < 6; ++k) out->partition_ranges[k] = s.ranges[k];
     out->overflow = s.n_instances > static_cast<unsigned long long>(ctx->fp.cap) ? 1 : 0;
-    out->end_bit = ctx->fp.end_bit;
+    out->end_bit = ctx->geo[view].end_bit;
+    out->n_instances_stored = static_cast<int64_t>(s.n_instances);
     return FHTGS_OK;
 }
 
@@ -518,24 +530,47 @@ fhtgs_status fhtgs_copy_intermediates(fhtgs_context ctx, int32_t view, fhtgs_int
     if (out->tile_type_partitioned && na)
         FHTGS_CK(cudaMemcpy(out->tile_type_partitioned, fb.tile_type_part + static_cast<size_t>(view) * fp.max_tiles, na,
                             cudaMemcpyDeviceToHost));
-    const size_t M = static_cast<size_t>(std::min<unsigned long long>(s.n_instances, static_cast<unsigned long long>(fp.cap)));
-    if (out->keys && M) {
-        if (fp.key_u32) {
-            FHTGS_CK(cudaMemcpy(out->keys, static_cast<uint32_t*>(fb.keys[fb.final_buf]) + static_cast<size_t>(view) * fp.cap,
-                                4 * M, cudaMemcpyDeviceToHost));
-        } else {
-            std::vector<uint16_t> k(M);
-            FHTGS_CK(cudaMemcpy(k.data(), static_cast<uint16_t*>(fb.keys[fb.final_buf]) + static_cast<size_t>(view) * fp.cap,
-                                2 * M, cudaMemcpyDeviceToHost));
-            for (size_t i = 0; i < M; ++i) out->keys[i] = k[i];
+    // Stored instances: one per (primitive, visible large tile), sorted by large tile.
+    const ViewGeom& g = ctx->geo[view];
+    const size_t Ms = static_cast<size_t>(std::min<unsigned long long>(s.n_instances, static_cast<unsigned long long>(fp.cap)));
+    std::vector<uint32_t> vals(Ms);
+    std::vector<uint2> lr(static_cast<size_t>(g.n_large));
+    if (Ms) FHTGS_CK(cudaMemcpy(vals.data(), fb.vals[fb.final_buf] + static_cast<size_t>(view) * fp.cap, 4 * Ms,
+                                cudaMemcpyDeviceToHost));
+    FHTGS_CK(cudaMemcpy(lr.data(), fb.ranges + static_cast<size_t>(view) * fp.max_large, 8 * lr.size(),
+                        cudaMemcpyDeviceToHost));
+    std::vector<uint8_t> lt(static_cast<size_t>(g.n_large));
+    FHTGS_CK(cudaMemcpy(lt.data(), fb.large_type + static_cast<size_t>(view) * fp.max_large, lt.size(),
+                        cudaMemcpyDeviceToHost));
+    // The reference's arrays (create_instances_cu + SortPairs + extract_instance_ranges_cu):
+    // keys are small-tile ids 4*t+i, the list of a fovea-circle tile (type fovea or blended) is
+    // repeated for its four sub-tiles, other visible tiles carry key 4*t once; the slots its
+    // area tables over-count follow as sentinel keys, up to its instance count.
+    const uint64_t m_ref = s.n_instances_ref;
+    const uint32_t sentinel = g.end_bit <= 16 ? 0xFFFFu : 0xFFFFFFFFu;
+    uint64_t pos = 0;
+    std::vector<uint2> rr(T, make_uint2(0, 0));
+    for (int t = 0; t < g.n_large; ++t) {
+        const uint2 r = lr[t];
+        if (r.y <= r.x) continue;
+        const uint32_t len = r.y - r.x;
+        const int reps = (lt[t] == kFovea || lt[t] == kBlended) ? kSubTiles : 1;
+        for (int i = 0; i < reps; ++i) {
+            const uint32_t key = static_cast<uint32_t>(t) * kSubTiles + i;
+            if (pos + len > m_ref) return fail(FHTGS_ERR_CAPACITY, "stored instances exceed the reference count");
+            for (uint32_t j = 0; j < len; ++j) {
+                if (out->keys) out->keys[pos + j] = key;
+                if (out->values) out->values[pos + j] = vals[r.x + j];
+            }
+            rr[key] = make_uint2(static_cast<uint32_t>(pos), static_cast<uint32_t>(pos + len));
+            pos += len;
         }
     }
-    if (out->values && M)
-        FHTGS_CK(cudaMemcpy(out->values, fb.vals[fb.final_buf] + static_cast<size_t>(view) * fp.cap, 4 * M,
-                            cudaMemcpyDeviceToHost));
-    if (out->instance_ranges && T)
-        FHTGS_CK(cudaMemcpy(out->instance_ranges, fb.ranges + static_cast<size_t>(view) * fp.max_tiles, 8 * T,
-                            cudaMemcpyDeviceToHost));
+    for (; pos < m_ref; ++pos) {
+        if (out->keys) out->keys[pos] = sentinel;
+        if (out->values) out->values[pos] = 0xFFFFFFFFu;
+    }
+    if (out->instance_ranges && T) std::memcpy(out->instance_ranges, rr.data(), 8 * T);
     return FHTGS_OK;
 }
 

@@ -6,10 +6,13 @@
 //   setup      gather per-view camera matrices into ViewParams
 //   classify   large-tile classification + compaction (one block per view)
 //   preprocess one thread per Gaussian for all views: cull, project, bounds, SH colour
-//   scan       exclusive scan of the preprocess blocks' touched-tile sums -> M per view
-//   create     tile|sub-tile keys + primitive values, sentinel fill of over-counted slots
+//   scan       exclusive scan of the preprocess blocks' instance sums -> M per view
+//   create     one (large-tile key, primitive) instance per visible tile of the bounds
 //   sort       stable LSD radix sort of (key, value) pairs, 8-bit digits
-//   ranges     [begin, end) per small tile from key boundaries
+//   ranges     [begin, end) per large tile from key boundaries
+// The reference stores the four sub-tiles of every fovea tile as separate instances with
+// identical lists, plus sentinel slots for masked fovea tiles; here each list is stored once
+// and the reference's arrays are reproduced exactly on request (fhtgs_copy_intermediates).
 //   blend      K-buffer blend; full-res 16x16 tiles (fovea, blended) and 2x-down 16x16
 //              tiles (periphery), persistent blocks pulling tiles from a work counter
 //   compose    periphery bilinear upsampling / blur and blended-ring cross-fade
@@ -182,6 +185,7 @@ __global__ void __launch_bounds__(1024) classify_kernel(FrameParams fp, FrameBuf
         st.n_masked_large = none ? nM + nP : nM;
         st.overflow = 0;
         st.n_instances = 0;
+        st.n_instances_ref = 0;
     }
 }
 
@@ -248,7 +252,9 @@ __device__ __forceinline__ float3 sh_to_rgb(const float* __restrict__ sh0, const
     return res;
 }
 
-__device__ __forceinline__ uint32_t touched_from_bounds(const ViewParams& vp, const uint4 b) {
+// Touched-tile count of the reference (visible tiles of the bounds from the visibility SAT,
+// plus 3 per fovea-window tile from the fovea SAT); `vis` receives the first part alone.
+__device__ __forceinline__ uint32_t touched_from_bounds(const ViewParams& vp, const uint4 b, uint32_t& vis) {
     const int diam = 2 * kFoveaRadiusTiles;
     const int tlx = vp.gaze_tiles_i.x - kFoveaRadiusTiles, tly = vp.gaze_tiles_i.y - kFoveaRadiusTiles;
     const uint4 fb = make_uint4(min(diam, max(0, static_cast<int>(b.x) - tlx)), min(diam, max(0, static_cast<int>(b.y) - tlx)),
@@ -256,6 +262,7 @@ __device__ __forceinline__ uint32_t touched_from_bounds(const ViewParams& vp, co
     const uint32_t W1 = static_cast<uint32_t>(vp.glw) + 1u;
     const uint32_t* sat = vp.vis_sat;
     uint32_t n = sat[b.y + W1 * b.w] + sat[b.x + W1 * b.z] - sat[b.y + W1 * b.z] - sat[b.x + W1 * b.w];
+    vis = n;
     if (fb.y != fb.x && fb.w != fb.z) {
         const uint32_t F1 = static_cast<uint32_t>(diam) + 1u;
         const uint32_t* f = vp.fovea_sat;
@@ -277,7 +284,7 @@ __device__ __forceinline__ float3 scaled_axis(float a, float b, float c, float s
 // Standard (non anti-aliased) transform and cull.  Returns true when culled.
 __device__ __forceinline__ bool transform_and_cull(const ViewParams& vp, const FrameParams& fp, float3 pos,
                                                    float3 scale, float4 quat, float opacity, float4& P1,
-                                                   float4& P2, float4& P4, uint4& b, uint32_t& n) {
+                                                   float4& P2, float4& P4, uint4& b, uint32_t& n, uint32_t& vis) {
     const float4 M3 = vp.M[2];
     const float z = dot(xyz(M3), pos) + M3.w;
     if (z < fp.near_plane || z > fp.far_plane) return true;
@@ -307,7 +314,7 @@ __device__ __forceinline__ bool transform_and_cull(const ViewParams& vp, const F
                    min(gw, static_cast<uint32_t>(max(0, __float2int_ru((cx + ex + 0.5f) / tw)))),
                    min(gh, static_cast<uint32_t>(max(0, __float2int_rd((cy - ey + 0.5f) / tw)))),
                    min(gh, static_cast<uint32_t>(max(0, __float2int_ru((cy + ey + 0.5f) / tw)))));
-    n = touched_from_bounds(vp, b);
+    n = touched_from_bounds(vp, b, vis);
     return n == 0;
 }
 
@@ -398,7 +405,7 @@ __device__ __forceinline__ float2 aabb_theta(float4 MT_axis, float4 MT3, float4 
 
 __device__ __forceinline__ bool transform_and_cull_aaa(const ViewParams& vp, const FrameParams& fp, float3 pos,
                                                        float3 osc, float4 quat, float& opacity, float4& P1,
-                                                       float4& P2, float4& P4, uint4& b, uint32_t& n) {
+                                                       float4& P2, float4& P4, uint4& b, uint32_t& n, uint32_t& vis) {
     const Mat3 R = quat_to_rot(quat);
     const float4 M3 = vp.M[2];
     const float z = dot(xyz(M3), pos) + M3.w;
@@ -450,7 +457,7 @@ __device__ __forceinline__ bool transform_and_cull_aaa(const ViewParams& vp, con
                    min(gw, static_cast<uint32_t>(max(0, __float2int_ru((ctr.x + ext.x) / tw)))),
                    min(gh, static_cast<uint32_t>(max(0, __float2int_rd((ctr.y - ext.y) / tw)))),
                    min(gh, static_cast<uint32_t>(max(0, __float2int_ru((ctr.y + ext.y) / tw)))));
-    n = touched_from_bounds(vp, b);
+    n = touched_from_bounds(vp, b, vis);
     return n == 0;
 }
 
@@ -471,16 +478,17 @@ __global__ void __launch_bounds__(kPrimBlock) preprocess_kernel(FrameParams fp, 
     const size_t N = static_cast<size_t>(fp.n_prims);
     for (int v = 0; v < fp.n_views; ++v) {
         const ViewParams& vp = fb.views[v];
-        uint32_t n = 0;
+        uint32_t n = 0, vis = 0;
         if (valid) {
             float4 P1, P2, P4;
             uint4 b;
             float opacity = op;
-            const bool culled = fp.aaa ? transform_and_cull_aaa(vp, fp, pos, scale, quat, opacity, P1, P2, P4, b, n)
-                                       : transform_and_cull(vp, fp, pos, scale, quat, opacity, P1, P2, P4, b, n);
-            if (culled) n = 0;
+            const bool culled = fp.aaa ? transform_and_cull_aaa(vp, fp, pos, scale, quat, opacity, P1, P2, P4, b, n, vis)
+                                       : transform_and_cull(vp, fp, pos, scale, quat, opacity, P1, P2, P4, b, n, vis);
+            if (culled) n = vis = 0;
             const size_t o = static_cast<size_t>(v) * N + ii;
             fb.n_touched[o] = n;
+            fb.n_vis[o] = vis;
             if (!culled) {
                 fb.bounds[o] = make_ushort4(static_cast<unsigned short>(b.x), static_cast<unsigned short>(b.y),
                                             static_cast<unsigned short>(b.z), static_cast<unsigned short>(b.w));
@@ -494,9 +502,13 @@ __global__ void __launch_bounds__(kPrimBlock) preprocess_kernel(FrameParams fp, 
                 r[3] = make_float4(rgb.x, rgb.y, rgb.z, opacity);
             }
         }
-        uint32_t tot;
-        block_excl_scan<uint32_t>(n, tot, s_warp);
-        if (threadIdx.x == 0) fb.block_sums[static_cast<size_t>(v) * fp.n_blocks_prim + blockIdx.x] = tot;
+        uint32_t tot_vis, tot_ref;
+        block_excl_scan<uint32_t>(vis, tot_vis, s_warp);
+        block_excl_scan<uint32_t>(n, tot_ref, s_warp);
+        if (threadIdx.x == 0) {
+            fb.block_sums[static_cast<size_t>(v) * fp.n_blocks_prim + blockIdx.x] = tot_vis;
+            atomicAdd(&fb.status[v].n_instances_ref, static_cast<unsigned long long>(tot_ref));
+        }
     }
 }
 
@@ -535,17 +547,14 @@ int launch_scan_blocks(const FrameParams& fp, const FrameBuffers& fb, cudaStream
 }
 
 // ------------------------------------------------------------------------------------------
-// instance creation (restates create_instances_cu, shared_kernels.cuh:15-130: keys
-// tile*4 (+sub-tile for fovea tiles) in row-major bbox order, values = primitive index; the
-// slots the area tables over-count keep the sentinel key, as the reference's 0xFF memset)
+// instance creation: one (large-tile key, primitive index) pair per visible large tile of a
+// primitive's bounds, in row-major bounds order (the emission order of create_instances_cu,
+// shared_kernels.cuh:15-130, with the reference's four sub-tile copies of a fovea tile folded
+// into one and no sentinel slots: the count per primitive is the visibility-SAT part of the
+// reference's touched-tile count)
 // ------------------------------------------------------------------------------------------
-constexpr uint32_t kSeqTiles = 16;   // bbox tiles handled by the owning thread
+constexpr uint32_t kSeqTiles = 16;   // bounds tiles handled by the owning thread
 constexpr int kBigList = kPrimBlock;
-
-template <typename KeyT>
-__device__ __forceinline__ void emit(KeyT* keys, uint32_t* vals, uint64_t pos, uint64_t lim, KeyT key, uint32_t val) {
-    if (pos < lim) { keys[pos] = key; vals[pos] = val; }
-}
 
 template <typename KeyT>
 __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParams fp, FrameBuffers fb) {
@@ -553,87 +562,71 @@ __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParam
     __shared__ uint32_t s_big_n;
     __shared__ uint32_t s_big_prim[kBigList];
     __shared__ uint32_t s_big_off[kBigList];
-    __shared__ uint32_t s_big_cnt[kBigList];
     __shared__ ushort4 s_big_b[kBigList];
     const int v = blockIdx.y;
     const ViewParams& vp = fb.views[v];
     const int i = blockIdx.x * kPrimBlock + threadIdx.x;
     const size_t N = static_cast<size_t>(fp.n_prims);
     const size_t o = static_cast<size_t>(v) * N + i;
-    const uint32_t nt = i < fp.n_prims ? fb.n_touched[o] : 0u;
+    const uint32_t nv = i < fp.n_prims ? fb.n_vis[o] : 0u;
     uint32_t tot;
-    const uint32_t local = block_excl_scan<uint32_t>(nt, tot, s_warp);
+    const uint32_t local = block_excl_scan<uint32_t>(nv, tot, s_warp);
     const uint32_t off = fb.block_sums[static_cast<size_t>(v) * fp.n_blocks_prim + blockIdx.x] + local;
     const uint64_t lim = static_cast<uint64_t>(fp.cap);
     KeyT* keys = reinterpret_cast<KeyT*>(fb.keys[0]) + static_cast<size_t>(v) * fp.cap;
     uint32_t* vals = fb.vals[0] + static_cast<size_t>(v) * fp.cap;
-    const KeyT sentinel = static_cast<KeyT>(~KeyT(0));
     const uint32_t glw = static_cast<uint32_t>(vp.glw);
     if (threadIdx.x == 0) s_big_n = 0;
     __syncthreads();
-    ushort4 b = make_ushort4(0, 0, 0, 0);
-    if (nt > 0) {
-        b = fb.bounds[o];
+    if (nv > 0) {
+        const ushort4 b = fb.bounds[o];
         const uint32_t bw = static_cast<uint32_t>(b.y - b.x);
         const uint32_t cnt = static_cast<uint32_t>(b.w - b.z) * bw;
         if (cnt <= kSeqTiles) {
             uint64_t w = off;
-            const uint64_t end = static_cast<uint64_t>(off) + nt;
-            for (uint32_t k = 0; k < cnt; ++k) {
-                const uint32_t tx = b.x + k % bw, ty = b.z + k / bw;
-                const uint32_t tile = ty * glw + tx;
+            const uint64_t end = static_cast<uint64_t>(off) + nv;
+            for (uint32_t k = 0; k < cnt && w < end; ++k) {
+                const uint32_t tile = (b.z + k / bw) * glw + b.x + k % bw;
                 if (!tile_visible(vp.vis_mask, tile)) continue;
-                const KeyT key = static_cast<KeyT>(tile * kSubTiles);
-                if (in_fovea<kFoveaRadiusTiles>(tx, ty, vp.gaze_tiles)) {
-                    for (int r = 0; r < kSubTiles; ++r, ++w)
-                        if (w < end) emit<KeyT>(keys, vals, w, lim, static_cast<KeyT>(key + r), static_cast<uint32_t>(i));
-                } else {
-                    if (w < end) emit<KeyT>(keys, vals, w, lim, key, static_cast<uint32_t>(i));
-                    ++w;
+                if (w < lim) {
+                    keys[w] = static_cast<KeyT>(tile);
+                    vals[w] = static_cast<uint32_t>(i);
                 }
+                ++w;
             }
-            for (; w < end; ++w) emit<KeyT>(keys, vals, w, lim, sentinel, static_cast<uint32_t>(i));
         } else {
             const uint32_t slot = atomicAdd(&s_big_n, 1u);
             s_big_prim[slot] = static_cast<uint32_t>(i);
             s_big_off[slot] = off;
-            s_big_cnt[slot] = nt;
             s_big_b[slot] = b;
         }
     }
     __syncthreads();
-    // Large footprints: the whole block walks the bounding box, 256 tiles per step, with a
-    // block scan of the per-tile instance counts giving each tile's slots.
+    // Large bounds: the whole block walks them, 256 tiles per step, a block scan of the
+    // per-tile visibility giving each visible tile its slot.
     const uint32_t n_big = s_big_n;
     for (uint32_t q = 0; q < n_big; ++q) {
         const uint32_t prim = s_big_prim[q];
         const ushort4 bb = s_big_b[q];
         const uint32_t bw = static_cast<uint32_t>(bb.y - bb.x);
         const uint32_t cnt = static_cast<uint32_t>(bb.w - bb.z) * bw;
-        const uint64_t end = static_cast<uint64_t>(s_big_off[q]) + s_big_cnt[q];
         uint64_t w0 = s_big_off[q];
         for (uint32_t base = 0; base < cnt; base += kPrimBlock) {
             const uint32_t k = base + threadIdx.x;
-            uint32_t c = 0, tile = 0;
-            bool fov = false;
+            uint32_t tile = 0, c = 0;
             if (k < cnt) {
-                const uint32_t tx = bb.x + k % bw, ty = bb.z + k / bw;
-                tile = ty * glw + tx;
-                if (tile_visible(vp.vis_mask, tile)) {
-                    fov = in_fovea<kFoveaRadiusTiles>(tx, ty, vp.gaze_tiles);
-                    c = fov ? kSubTiles : 1;
-                }
+                tile = (bb.z + k / bw) * glw + bb.x + k % bw;
+                c = tile_visible(vp.vis_mask, tile) ? 1u : 0u;
             }
             uint32_t step;
             const uint32_t ex = block_excl_scan<uint32_t>(c, step, s_warp);
-            const KeyT key = static_cast<KeyT>(tile * kSubTiles);
-            for (uint32_t r = 0; r < c; ++r) {
-                const uint64_t w = w0 + ex + r;
-                if (w < end) emit<KeyT>(keys, vals, w, lim, static_cast<KeyT>(key + r), prim);
+            const uint64_t w = w0 + ex;
+            if (c && w < lim) {
+                keys[w] = static_cast<KeyT>(tile);
+                vals[w] = prim;
             }
             w0 += step;
         }
-        for (uint64_t w = w0 + threadIdx.x; w < end; w += kPrimBlock) emit<KeyT>(keys, vals, w, lim, sentinel, prim);
     }
 }
 
@@ -666,12 +659,13 @@ __global__ void __launch_bounds__(kSortThreads) sort_upsweep_kernel(FrameParams 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int k = threadIdx.x; k < (kSortThreads / 32) * kSortBins; k += kSortThreads) (&s_hist[0][0])[k] = 0;
     __syncthreads();
-    const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[buf]) + static_cast<size_t>(v) * fp.cap;
-    const uint64_t wbase = t0 + static_cast<uint64_t>(warp) * 32 * kSortItems;
+    const uint32_t n_here = static_cast<uint32_t>(M - t0 < static_cast<uint64_t>(kSortTile) ? M - t0 : kSortTile);
+    const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[buf]) + static_cast<size_t>(v) * fp.cap + t0;
+    const uint32_t wbase = static_cast<uint32_t>(warp) * 32 * kSortItems + lane;
 #pragma unroll 4
     for (int it = 0; it < kSortItems; ++it) {
-        const uint64_t idx = wbase + static_cast<uint64_t>(it) * 32 + lane;
-        const bool ok = idx < M;
+        const uint32_t idx = wbase + it * 32;
+        const bool ok = idx < n_here;
         const uint32_t d = ok ? (static_cast<uint32_t>(keys[idx]) >> shift) & (kSortBins - 1) : kSortBins;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         if (ok && lane == __ffs(peers) - 1) s_hist[warp][d] += __popc(peers);
@@ -704,8 +698,8 @@ __global__ void __launch_bounds__(256) sort_scan_kernel(FrameParams fp, FrameBuf
 }
 
 template <typename KeyT>
-__global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(FrameParams fp, FrameBuffers fb, int buf, int shift) {
-    __shared__ uint32_t s_whist[kSortThreads / 32][kSortBins];  // per-warp counts -> per-warp prefix
+__global__ void __launch_bounds__(kSortThreads, 3) sort_scatter_kernel(FrameParams fp, FrameBuffers fb, int buf, int shift) {
+    __shared__ uint32_t s_whist[kSortThreads / 32][kSortBins];  // per-warp counts, then running slots
     __shared__ uint32_t s_local_start[kSortBins];
     __shared__ uint32_t s_global_start[kSortBins];
     __shared__ uint32_t s_warp[33];
@@ -719,59 +713,63 @@ __global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(FrameParams 
     const uint32_t lanemask_lt = (1u << lane) - 1u;
     for (int k = threadIdx.x; k < (kSortThreads / 32) * kSortBins; k += kSortThreads) (&s_whist[0][0])[k] = 0;
     __syncthreads();
-    const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[buf]) + static_cast<size_t>(v) * fp.cap;
-    const uint32_t* vals = fb.vals[buf] + static_cast<size_t>(v) * fp.cap;
+    const uint32_t n_here = static_cast<uint32_t>(M - t0 < static_cast<uint64_t>(kSortTile) ? M - t0 : kSortTile);
+    const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[buf]) + static_cast<size_t>(v) * fp.cap + t0;
+    const uint32_t* vals = fb.vals[buf] + static_cast<size_t>(v) * fp.cap + t0;
     KeyT* okeys = reinterpret_cast<KeyT*>(fb.keys[buf ^ 1]) + static_cast<size_t>(v) * fp.cap;
     uint32_t* ovals = fb.vals[buf ^ 1] + static_cast<size_t>(v) * fp.cap;
-    const uint64_t wbase = t0 + static_cast<uint64_t>(warp) * 32 * kSortItems;
+    // Each warp owns 32 * kSortItems consecutive keys, visited warp-striped (coalesced loads);
+    // the visit order is the key order, which makes the ranking stable.
+    const uint32_t wbase = static_cast<uint32_t>(warp) * 32 * kSortItems + lane;
     KeyT k_reg[kSortItems];
     uint32_t v_reg[kSortItems];
-    uint32_t rank[kSortItems];
 #pragma unroll
     for (int it = 0; it < kSortItems; ++it) {
-        const uint64_t idx = wbase + static_cast<uint64_t>(it) * 32 + lane;
-        const bool ok = idx < M;
+        const uint32_t idx = wbase + it * 32;
+        const bool ok = idx < n_here;
         k_reg[it] = ok ? keys[idx] : static_cast<KeyT>(0);
         v_reg[it] = ok ? vals[idx] : 0u;
         const uint32_t d = ok ? (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1) : kSortBins;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        const uint32_t before = ok ? s_whist[warp][d] : 0u;
-        rank[it] = before + __popc(peers & lanemask_lt);
-        __syncwarp();
-        if (ok && lane == __ffs(peers) - 1) s_whist[warp][d] = before + __popc(peers);
+        if (ok && lane == __ffs(peers) - 1) s_whist[warp][d] += __popc(peers);
         __syncwarp();
     }
     __syncthreads();
-    // per-digit: exclusive prefix over warps, tile count, local start (scan over digits)
+    // digit d (thread d): counts of the warps -> exclusive prefix, tile count, starts
     const int d = threadIdx.x;
-    uint32_t cnt = 0;
+    uint32_t cnt = 0, wpre[kSortThreads / 32];
 #pragma unroll
     for (int w = 0; w < kSortThreads / 32; ++w) {
-        const uint32_t c = s_whist[w][d];
-        s_whist[w][d] = cnt;
-        cnt += c;
+        wpre[w] = cnt;
+        cnt += s_whist[w][d];
     }
     uint32_t tile_total;
     const uint32_t lstart = block_excl_scan<uint32_t>(cnt, tile_total, s_warp);
     s_local_start[d] = lstart;
-    // global start of digit d for this tile: exclusive scan of digit totals + tile offset
     const uint32_t dtot = fb.sort_digit_tot[static_cast<size_t>(v) * kSortBins + d];
     uint32_t all_total;
     const uint32_t dbase = block_excl_scan<uint32_t>(dtot, all_total, s_warp);
     s_global_start[d] = dbase + fb.sort_hist[(static_cast<size_t>(v) * kSortBins + d) * fb.sort_tiles + blockIdx.x];
+#pragma unroll
+    for (int w = 0; w < kSortThreads / 32; ++w) s_whist[w][d] = lstart + wpre[w];  // first slot of warp w
     __syncthreads();
+    // second visit: stable slot of every key inside the tile
 #pragma unroll
     for (int it = 0; it < kSortItems; ++it) {
-        const uint64_t idx = wbase + static_cast<uint64_t>(it) * 32 + lane;
-        if (idx < M) {
-            const uint32_t dd = (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1);
-            const uint32_t p = s_local_start[dd] + s_whist[warp][dd] + rank[it];
+        const bool ok = wbase + it * 32 < n_here;
+        const uint32_t dd = ok ? (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1) : kSortBins;
+        const uint32_t peers = __match_any_sync(0xffffffffu, dd);
+        const uint32_t base = ok ? s_whist[warp][dd] : 0u;
+        __syncwarp();
+        if (ok) {
+            const uint32_t p = base + __popc(peers & lanemask_lt);
             s_keys[p] = k_reg[it];
             s_vals[p] = v_reg[it];
+            if (lane == __ffs(peers) - 1) s_whist[warp][dd] = base + __popc(peers);
         }
+        __syncwarp();
     }
     __syncthreads();
-    const uint32_t n_here = static_cast<uint32_t>(M - t0 < static_cast<uint64_t>(kSortTile) ? M - t0 : kSortTile);
     for (uint32_t j = threadIdx.x; j < n_here; j += kSortThreads) {
         const KeyT kk = s_keys[j];
         const uint32_t dd = (static_cast<uint32_t>(kk) >> shift) & (kSortBins - 1);
@@ -803,39 +801,139 @@ int launch_sort(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------------------------------------
-// per-small-tile instance ranges (restates extract_instance_ranges_cu,
-// shared_kernels.cuh:133-152; ranges are zeroed beforehand)
+// per-large-tile instance ranges from the boundaries of the sorted keys (the boundary rule of
+// extract_instance_ranges_cu, shared_kernels.cuh:133-152; ranges are zeroed beforehand)
 // ------------------------------------------------------------------------------------------
 template <typename KeyT>
-__global__ void ranges_kernel(FrameParams fp, FrameBuffers fb) {
+__global__ void __launch_bounds__(256) ranges_kernel(FrameParams fp, FrameBuffers fb) {
     const int v = blockIdx.y;
     const uint64_t M = view_count(fp, fb, v);
-    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= M) return;
     const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[fb.final_buf]) + static_cast<size_t>(v) * fp.cap;
-    uint2* r = fb.ranges + static_cast<size_t>(v) * fp.max_tiles;
-    const KeyT sentinel = static_cast<KeyT>(~KeyT(0));
-    const KeyT k = keys[i];
-    if (i == 0) {
-        if (k != sentinel) r[k].x = 0;
-    } else {
-        const KeyT prev = keys[i - 1];
-        if (k != prev) {
-            if (prev != sentinel) r[prev].y = static_cast<uint32_t>(i);
-            if (k != sentinel) r[k].x = static_cast<uint32_t>(i);
+    uint2* r = fb.ranges + static_cast<size_t>(v) * fp.max_large;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < M;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const KeyT k = keys[i];
+        if (i == 0) {
+            r[k].x = 0;
+        } else {
+            const KeyT prev = keys[i - 1];
+            if (k != prev) {
+                r[prev].y = static_cast<uint32_t>(i);
+                r[k].x = static_cast<uint32_t>(i);
+            }
         }
+        if (i == M - 1) r[k].y = static_cast<uint32_t>(M);
     }
-    if (i == M - 1 && k != sentinel) r[k].y = static_cast<uint32_t>(M);
 }
 
-int launch_ranges(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s) {
-    cudaMemsetAsync(fb.ranges, 0, sizeof(uint2) * static_cast<size_t>(fp.max_tiles) * fp.n_views, s);
+int launch_ranges(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s) {
+    cudaMemsetAsync(fb.ranges, 0, sizeof(uint2) * static_cast<size_t>(fp.max_large) * fp.n_views, s);
     if (fb.sort_tiles == 0) return 0;
-    const unsigned nb = static_cast<unsigned>((fp.cap + 255) / 256);
+    const int64_t want = (fp.cap + 255) / 256;
+    const unsigned nb = static_cast<unsigned>(want < 8 * n_sms ? (want > 0 ? want : 1) : 8 * n_sms);
     dim3 grid(nb, fp.n_views);
     if (fp.key_u32) ranges_kernel<uint32_t><<<grid, 256, 0, s>>>(fp, fb);
     else ranges_kernel<uint16_t><<<grid, 256, 0, s>>>(fp, fb);
     return 1;
+}
+
+// ------------------------------------------------------------------------------------------
+// work ordering for the persistent blend (bucketed longest-processing-time first)
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ int list_count(const FrameStatus& st, int list) {
+    return list == 0 ? static_cast<int>(st.n_fovea_large + st.n_blended_large) : static_cast<int>(st.n_periphery_large);
+}
+
+__device__ __forceinline__ int cost_bucket(uint32_t len) {
+    return len == 0 ? 0 : min(kOrderBuckets - 1, 1 + __float2int_rd(4.0f * __log2f(static_cast<float>(len))));
+}
+
+// Maps flat item g of `list` to (view, item within the view); `pre` holds the exclusive prefix
+// of the per-view counts.
+__device__ __forceinline__ void item_of(int g, const int* pre, int n_views, int& v, int& j) {
+    int lo = 0, hi = n_views - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= g) lo = mid; else hi = mid - 1;
+    }
+    v = lo;
+    j = g - pre[lo];
+}
+
+__device__ __forceinline__ uint32_t item_len(const FrameParams& fp, const FrameBuffers& fb, int list, int v, int j) {
+    const uint32_t lt = list == 0 ? fb.work_full[static_cast<size_t>(v) * fp.max_large + j]
+                                  : fb.work_low[static_cast<size_t>(v) * fp.max_large + j];
+    const uint2 r = fb.ranges[static_cast<size_t>(v) * fp.max_large + lt];
+    return r.y > r.x ? r.y - r.x : 0u;
+}
+
+constexpr int kMaxOrderViews = 1024;
+
+// Per-view prefix of the list counts into shared memory; returns the total.
+__device__ __forceinline__ int list_prefix(const FrameParams& fp, const FrameBuffers& fb, int list, int* pre) {
+    __shared__ int s_total;
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int v = 0; v < fp.n_views; ++v) {
+            pre[v] = acc;
+            acc += list_count(fb.status[v], list);
+        }
+        s_total = acc;
+    }
+    __syncthreads();
+    return s_total;
+}
+
+__global__ void __launch_bounds__(256) order_hist_kernel(FrameParams fp, FrameBuffers fb) {
+    __shared__ int pre[kMaxOrderViews];
+    __shared__ uint32_t hist[kOrderBuckets];
+    const int list = blockIdx.y;
+    const int total = list_prefix(fp, fb, list, pre);
+    for (int k = threadIdx.x; k < kOrderBuckets; k += blockDim.x) hist[k] = 0;
+    __syncthreads();
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        int v, j;
+        item_of(g, pre, fp.n_views, v, j);
+        atomicAdd(&hist[cost_bucket(item_len(fp, fb, list, v, j))], 1u);
+    }
+    __syncthreads();
+    uint32_t* gh = fb.counters + 4 + list * kOrderBuckets;
+    for (int k = threadIdx.x; k < kOrderBuckets; k += blockDim.x)
+        if (hist[k]) atomicAdd(&gh[k], hist[k]);
+}
+
+__global__ void __launch_bounds__(256) order_scatter_kernel(FrameParams fp, FrameBuffers fb) {
+    __shared__ int pre[kMaxOrderViews];
+    __shared__ uint32_t base[kOrderBuckets];
+    const int list = blockIdx.y;
+    const int total = list_prefix(fp, fb, list, pre);
+    const uint32_t* gh = fb.counters + 4 + list * kOrderBuckets;
+    uint32_t* cursor = fb.counters + 4 + 2 * kOrderBuckets + list * kOrderBuckets;
+    if (threadIdx.x == 0) {  // descending bucket order
+        uint32_t acc = 0;
+        for (int k = kOrderBuckets - 1; k >= 0; --k) {
+            base[k] = acc;
+            acc += gh[k];
+        }
+    }
+    __syncthreads();
+    uint32_t* out = fb.work_order[list];
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        int v, j;
+        item_of(g, pre, fp.n_views, v, j);
+        const int b = cost_bucket(item_len(fp, fb, list, v, j));
+        const uint32_t pos = base[b] + atomicAdd(&cursor[b], 1u);
+        out[pos] = (static_cast<uint32_t>(v) << 24) | static_cast<uint32_t>(j);
+    }
+}
+
+int launch_order(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s) {
+    const int per_list = fp.n_views * fp.max_large;
+    int blocks = (per_list + 255) / 256;
+    blocks = blocks < 2 * n_sms ? (blocks > 0 ? blocks : 1) : 2 * n_sms;
+    order_hist_kernel<<<dim3(blocks, 2), 256, 0, s>>>(fp, fb);
+    order_scatter_kernel<<<dim3(blocks, 2), 256, 0, s>>>(fp, fb);
+    return 2;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -951,11 +1049,66 @@ __device__ __forceinline__ bool cutoff_box(const float4 P1, const float4 P2, con
     return true;
 }
 
+// The cutoff ellipse of a Gaussian as a conic F(x', y') <= 0 about its projected mean
+// (x' = x - x0, y' = y - y0).  With Q1 = VPMT1 - x0 VPMT4 and Q2 = VPMT2 - y0 VPMT4 (both with
+// zero w) the blend's moment vector is m = w4 (y' q1 - x' q2) and its direction vector
+// d = q1 x q2 + x' (q2 x n4) + y' (n4 x q1), so rho^2 <= rc  <=>
+//   w4^2 |y' q1 - x' q2|^2 - rc |d|^2 <= 0.
+// rc is inflated by 2 % and the rectangles by half a pixel, far above float rounding, so a
+// rectangle reported empty holds no pixel the blend could accept.
+struct Conic {
+    float x0, y0, A, B, C, D, E, F0, det;
+};
+
+__device__ __forceinline__ bool cutoff_conic(const float4 P1, const float4 P2, const float4 P4, float opacity, Conic& q) {
+    const float rc = 2.0f * __logf(opacity * kMinAlphaRcp) * 1.02f;
+    const float3 n4 = xyz(P4);
+    const float w4 = P4.w;
+    if (!(rc > 0.0f) || !(w4 > 0.0f)) return false;
+    q.x0 = P1.w / w4;
+    q.y0 = P2.w / w4;
+    const float3 q1 = xyz(P1) - q.x0 * n4, q2 = xyz(P2) - q.y0 * n4;
+    const float3 c0 = cross(q1, q2), cx = cross(q2, n4), cy = cross(n4, q1);
+    const float ww = w4 * w4;
+    q.A = ww * dot(q2, q2) - rc * dot(cx, cx);
+    q.C = ww * dot(q1, q1) - rc * dot(cy, cy);
+    q.B = -2.0f * (ww * dot(q1, q2) + rc * dot(cx, cy));
+    q.D = -2.0f * rc * dot(c0, cx);
+    q.E = -2.0f * rc * dot(c0, cy);
+    q.F0 = -rc * dot(c0, c0);
+    q.det = 4.0f * q.A * q.C - q.B * q.B;
+    // an ellipse, clearly: positive definite quadratic part
+    return q.A > 0.0f && q.C > 0.0f && q.det > 1e-4f * (4.0f * q.A * q.C) && isfinite(q.det) && isfinite(q.F0) &&
+           isfinite(q.D) && isfinite(q.E) && isfinite(q.x0) && isfinite(q.y0);
+}
+
+// Does the ellipse F <= 0 meet the pixel rectangle [ax0, ax1] x [ay0, ay1]?  Minimum of the
+// convex F over the rectangle: the free minimum if it lies inside, else the best edge point.
+__device__ __forceinline__ bool conic_meets_rect(const Conic& q, float ax0, float ax1, float ay0, float ay1) {
+    const float X0 = ax0 - q.x0 - 0.5f, X1 = ax1 - q.x0 + 0.5f, Y0 = ay0 - q.y0 - 0.5f, Y1 = ay1 - q.y0 + 0.5f;
+    const float xc = (q.B * q.E - 2.0f * q.C * q.D) / q.det, yc = (q.B * q.D - 2.0f * q.A * q.E) / q.det;
+    if (xc >= X0 && xc <= X1 && yc >= Y0 && yc <= Y1) return true;
+    auto F = [&](float x, float y) { return (q.A * x + q.B * y + q.D) * x + (q.C * y + q.E) * y + q.F0; };
+    const float i2a = 0.5f / q.A, i2c = 0.5f / q.C;
+    const float yl = fminf(fmaxf(-(q.B * X0 + q.E) * i2c, Y0), Y1);
+    const float yr = fminf(fmaxf(-(q.B * X1 + q.E) * i2c, Y0), Y1);
+    const float xt = fminf(fmaxf(-(q.B * Y0 + q.D) * i2a, X0), X1);
+    const float xb = fminf(fmaxf(-(q.B * Y1 + q.D) * i2a, X0), X1);
+    const float m = fminf(fminf(F(X0, yl), F(X1, yr)), fminf(F(xt, Y0), F(xb, Y1)));
+    return !(m > 0.0f);
+}
+
 // One block renders one 16x16 area.  LOWRES: 64 threads sample it at stride 2 (periphery);
 // otherwise 256 threads render it at full resolution (fovea / blended).  Warp w covers an
 // 8-wide, 4-high block of samples.
+// Resident blocks per SM the register allocation has to allow: the K-buffer (2 K registers)
+// dominates for large K.
+__host__ __device__ constexpr int blend_min_blocks(int K, bool lowres) {
+    return lowres ? (K >= 32 ? 8 : K >= 16 ? 12 : 16) : (K >= 32 ? 2 : K >= 16 ? 3 : 4);
+}
+
 template <int K, bool LOWRES>
-__global__ void __launch_bounds__(LOWRES ? 64 : 256) blend_kernel(FrameParams fp, FrameBuffers fb, int counter_idx) {
+__global__ void __launch_bounds__(LOWRES ? 64 : 256, blend_min_blocks(K, LOWRES)) blend_kernel(FrameParams fp, FrameBuffers fb, int counter_idx) {
     constexpr int NT = LOWRES ? 64 : 256;
     constexpr int NW = NT / 32;
     constexpr int S = LOWRES ? kStride : 1;
@@ -970,23 +1123,17 @@ __global__ void __launch_bounds__(LOWRES ? 64 : 256) blend_kernel(FrameParams fp
     const int ly = (warp / WX) * 4 + (lane >> 3);
     // total work items over all views
     int total = 0;
-    for (int v = 0; v < fp.n_views; ++v) {
-        const FrameStatus& st = fb.status[v];
-        total += LOWRES ? static_cast<int>(st.n_periphery_large) : static_cast<int>(st.n_fovea_large + st.n_blended_large);
-    }
+    for (int v = 0; v < fp.n_views; ++v) total += list_count(fb.status[v], LOWRES ? 1 : 0);
+    const uint32_t* order = fb.work_order[LOWRES ? 1 : 0];
     for (;;) {
         if (tid == 0) s_item = static_cast<int>(atomicAdd(&fb.counters[counter_idx], 1u));
         __syncthreads();
-        int item = s_item;
+        const int g = s_item;
         __syncthreads();
-        if (item >= total) break;
-        int v = 0;
-        for (; v < fp.n_views; ++v) {
-            const FrameStatus& st = fb.status[v];
-            const int c = LOWRES ? static_cast<int>(st.n_periphery_large) : static_cast<int>(st.n_fovea_large + st.n_blended_large);
-            if (item < c) break;
-            item -= c;
-        }
+        if (g >= total) break;
+        const uint32_t packed = order[g];
+        const int v = static_cast<int>(packed >> 24);
+        const int item = static_cast<int>(packed & 0xFFFFFFu);
         const ViewParams& vp = fb.views[v];
         const FrameStatus& st = fb.status[v];
         const uint32_t lt = LOWRES ? fb.work_low[static_cast<size_t>(v) * fp.max_large + item]
@@ -998,7 +1145,7 @@ __global__ void __launch_bounds__(LOWRES ? 64 : 256) blend_kernel(FrameParams fp
         const bool inside = px_i < vp.width && py_i < vp.height;
         const float pixel_x = __uint2float_rn(static_cast<uint32_t>(px_i));
         const float pixel_y = __uint2float_rn(static_cast<uint32_t>(py_i));
-        const uint2 range = fb.ranges[static_cast<size_t>(v) * fp.max_tiles + lt * kSubTiles];
+        const uint2 range = fb.ranges[static_cast<size_t>(v) * fp.max_large + lt];
         const uint32_t* vals = fb.vals[fb.final_buf] + static_cast<size_t>(v) * fp.cap;
         const float4* rec = fb.rec + 4 * static_cast<size_t>(v) * fp.n_prims;
 
@@ -1025,12 +1172,16 @@ __global__ void __launch_bounds__(LOWRES ? 64 : 256) blend_kernel(FrameParams fp
                 if (cutoff_box(P1, P2, P4, c.w, box, never)) {
                     if (never) m = 0u;
                     else {
+                        Conic q;
+                        const bool ell = cutoff_conic(P1, P2, P4, c.w, q);
                         m = 0u;
 #pragma unroll
                         for (int w = 0; w < NW; ++w) {
                             const float ax0 = static_cast<float>(ox + (w % WX) * 8 * S), ax1 = ax0 + 7.0f * S;
                             const float ay0 = static_cast<float>(oy + (w / WX) * 4 * S), ay1 = ay0 + 3.0f * S;
-                            if (box.y >= ax0 && box.x <= ax1 && box.w >= ay0 && box.z <= ay1) m |= 1u << w;
+                            if (box.y >= ax0 && box.x <= ax1 && box.w >= ay0 && box.z <= ay1 &&
+                                (!ell || conic_meets_rect(q, ax0, ax1, ay0, ay1)))
+                                m |= 1u << w;
                         }
                     }
                 }
@@ -1307,8 +1458,8 @@ int launch_compose(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s
 }
 
 const KernelSet& kernel_set() {
-    static const KernelSet ks = {launch_setup,  launch_classify, launch_preprocess, launch_scan_blocks, launch_create,
-                                 launch_sort,   launch_ranges,   launch_blend,      launch_compose};
+    static const KernelSet ks = {launch_setup, launch_classify, launch_preprocess, launch_scan_blocks, launch_create,
+                                 launch_sort,  launch_ranges,   launch_order,      launch_blend,       launch_compose};
     return ks;
 }
 

@@ -70,7 +70,7 @@ struct FrameParams {
     const float* bg_data;
     int tex_w, tex_h;
     int key_u32;           // 0: 16-bit keys, 1: 32-bit keys
-    int end_bit;           // bits sorted (max over views)
+    int end_bit;           // key bits sorted: bit width of the largest large-tile index
     int64_t cap;           // instance slots per view
     int max_tiles;         // max small-tile ids over views (stride of per-tile arrays)
     int max_large;         // max large tiles over views
@@ -78,8 +78,12 @@ struct FrameParams {
 };
 
 // Per-view frame status written by the device, read by the host after the frame.
+// Instances are stored once per (primitive, visible large tile): `n_instances` counts those;
+// `n_instances_ref` is the reference's count (sum of touched-tile counts, with the four
+// sub-tiles of a fovea tile and the over-counted slots of masked fovea tiles).
 struct FrameStatus {
-    unsigned long long n_instances;   // M (64-bit sum)
+    unsigned long long n_instances;   // stored instances (sorted, blended)
+    unsigned long long n_instances_ref;
     uint32_t n_active;                // entries in the partitioned tile map
     uint32_t ranges[6];               // partition ranges (fovea, periphery, blended)
     uint32_t n_fovea_large, n_blended_large, n_periphery_large, n_masked_large;
@@ -101,7 +105,8 @@ struct Gaussians {
 struct FrameBuffers {
     ViewParams* views;
     FrameStatus* status;
-    uint32_t* n_touched;      // [V][N]
+    uint32_t* n_touched;      // [V][N] reference touched-tile counts
+    uint32_t* n_vis;          // [V][N] visible large tiles in the bounds = stored instances
     ushort4* bounds;          // [V][N]
     float4* rec;              // [V][N][4]: VPMT1, VPMT2, VPMT4, rgba
     uint32_t* block_sums;     // [V][n_blocks_prim]
@@ -111,15 +116,23 @@ struct FrameBuffers {
     uint32_t* sort_hist;      // [V][256][sort_tiles]
     uint32_t* sort_digit_tot; // [V][256]
     int sort_tiles;           // tiles of the radix sort per view (capacity based)
-    uint2* ranges;            // [V][max_tiles]
+    uint2* ranges;            // [V][max_large] instance range per large tile
     uint32_t* tile_map_part;  // [V][max_tiles]
     uint8_t* tile_type_part;  // [V][max_tiles]
     uint8_t* large_type;      // [V][max_large]
     uint32_t* work_full;      // [V][max_large] fovea then blended large tiles
     uint32_t* work_low;       // [V][max_large] periphery large tiles
     uint32_t* work_masked;    // [V][max_large] masked large tiles
-    uint32_t* counters;       // [4] persistent-kernel work counters
+    uint32_t* counters;       // [kCounterWords]: work counters, then the work-order buckets
+    uint32_t* work_order[2];  // [V*max_large] packed (view << 24 | item), heaviest first:
+                              // [0] fovea+blended tiles, [1] periphery tiles
 };
+
+// Work ordering: tiles are bucketed by list length in quarter octaves and blended in
+// descending bucket order, so that the longest lists start first (longest-processing-time
+// scheduling of the persistent blend blocks).
+constexpr int kOrderBuckets = 130;
+constexpr int kCounterWords = 4 + 2 * 2 * kOrderBuckets;  // counters, histograms, cursors
 
 // Launchers exported by each math flavour (fast = -use_fast_math, ieee = default).
 struct KernelSet {
@@ -130,7 +143,8 @@ struct KernelSet {
     int (*scan_blocks)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);
     int (*create_instances)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);
     int (*sort)(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s);
-    int (*ranges)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);
+    int (*ranges)(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s);
+    int (*order)(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s);
     // `mid` (may be null) is recorded between the full-resolution and the periphery blend.
     int (*blend)(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid);
     int (*compose)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);

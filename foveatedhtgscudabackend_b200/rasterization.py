@@ -370,7 +370,8 @@ class Renderer:
         _lib.check(self._libh.fhtgs_get_frame_info(self.ctx, view, C.byref(fi)))
         return dict(n_instances=int(fi.n_instances), instance_capacity=int(fi.instance_capacity),
                     n_active_tiles=int(fi.n_active_tiles), partition_ranges=list(fi.partition_ranges),
-                    overflow=bool(fi.overflow), end_bit=int(fi.end_bit))
+                    overflow=bool(fi.overflow), end_bit=int(fi.end_bit),
+                    n_instances_stored=int(fi.n_instances_stored))
 
     def intermediates(self, view: int = 0) -> dict:
         """Host copies of the last frame's per-primitive, tile and instance data of one view."""
@@ -380,7 +381,7 @@ class Renderer:
         n = self._last_n
         w, h = self._last_sizes[view]
         T = 4 * ((w + 15) // 16) * ((h + 15) // 16)
-        m = min(info["n_instances"], info["instance_capacity"])
+        m = info["n_instances"]
         na = info["n_active_tiles"]
         out = dict(n_touched=np.zeros(n, np.uint32), screen_bounds=np.zeros((n, 4), np.uint16),
                    vpmt=np.zeros((n, 12), np.float32), rgba=np.zeros((n, 4), np.float32),

@@ -91,16 +91,22 @@ typedef struct {
 
 /* Per-view facts of the last frame rendered by a context (read after it completed). */
 typedef struct {
-    int64_t n_instances;       /* M = sum of touched tiles (includes sentinel slots) */
-    int64_t instance_capacity; /* arena slots available per view                     */
-    uint32_t n_active_tiles;   /* small-tile entries in the tile index map           */
-    uint32_t partition_ranges[6]; /* fovea, periphery, blended [begin,end)           */
-    int32_t overflow;          /* 1 when n_instances > instance_capacity             */
-    int32_t end_bit;           /* key bits sorted                                   */
+    int64_t n_instances;       /* reference's M = sum of touched-tile counts (sub-tile copies
+                                  of fovea tiles and over-counted sentinel slots included) */
+    int64_t instance_capacity; /* stored-instance slots available per view                 */
+    uint32_t n_active_tiles;   /* small-tile entries in the tile index map                 */
+    uint32_t partition_ranges[6]; /* fovea, periphery, blended [begin,end)                 */
+    int32_t overflow;          /* 1 when n_instances_stored > instance_capacity             */
+    int32_t end_bit;           /* reference key bits (bit width of small tiles + 1)         */
+    int64_t n_instances_stored;/* instances actually stored and sorted: one per (Gaussian,
+                                  visible 16x16 tile)                                      */
 } fhtgs_frame_info;
 
-/* Intermediates of one view of the last frame, copied to HOST buffers (any may be NULL).
- * Keys are widened to uint32; sentinels are 0xFFFF (16-bit keys) or 0xFFFFFFFF. */
+/* Intermediates of one view of the last frame, copied to HOST buffers (any may be NULL), in
+ * the reference's layout: keys are small-tile ids widened to uint32, the list of a fovea-circle
+ * tile appears once per sub-tile, and over-counted slots follow as sentinel keys (0xFFFF for
+ * 16-bit keys, else 0xFFFFFFFF) with value 0xFFFFFFFF.  The renderer itself stores each list
+ * once; these arrays are expanded from it exactly. */
 typedef struct {
     uint32_t* n_touched;      /* [N]           */
     uint16_t* screen_bounds;  /* [N,4]         */

@@ -1,0 +1,80 @@
+"""Times the reference's own CUDA backend against libfhtgs on the same B200 — MEASUREMENT OF THE
+REFERENCE, test infrastructure (oracle/_ref must hold the reference build of oracle/build_ref.sh).
+
+Both sides are called through the same positional drop-in API (`_C_stereo.render`): the
+reference's module from oracle/_ref and this package's mirror.  Per call: CUDA events around the
+blocking call, 10 warm-up calls, then --calls timed calls; median and p99 in ms, frames/s from the
+median.  Also checks that the two produce identical images on the workload.
+
+    python oracle/time_ref_cuda.py [--calls 100] [--n 1000000] [--width 2064 --height 2208]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
+
+
+def timed_calls(fn, calls: int, warmup: int = 10):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(calls):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    ms = np.asarray(ms)
+    return {"median_ms": float(np.median(ms)), "p99_ms": float(np.percentile(ms, 99)),
+            "mean_ms": float(ms.mean()), "frames_per_s": float(1000.0 / np.median(ms)), "calls": calls}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--calls", type=int, default=100)
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--width", type=int, default=2064)
+    ap.add_argument("--height", type=int, default=2208)
+    ap.add_argument("--K", type=int, default=8)
+    a = ap.parse_args(argv)
+
+    import torch
+
+    import foveatedhtgscudabackend_b200 as F
+    from foveatedhtgscudabackend_b200 import scene
+    import ref as REF
+
+    g = scene.make_gaussians(a.n, 3, seed=0)
+    left, right = scene.make_stereo_views(a.width, a.height, seed=0)
+    gt = F.gaussians_to_torch(g)
+    st = [F.settings_from_view(v, K=a.K, active_sh_bases=16) for v in (left, right)]
+    args = (*gt, *st[0].as_tuple(), *st[1].as_tuple(), True, False, False)
+    ref_mod = REF.module("_C_stereo")
+    mine = F._C_stereo.render(*args)
+    theirs = ref_mod.render(*args)
+    torch.cuda.synchronize()
+    same = [bool(torch.equal(x, y)) for x, y in zip(mine, theirs)]
+    res = {
+        "workload": f"stereo {a.n} Gaussians SH3, 2x{a.width}x{a.height}, K={a.K}",
+        "reference_cuda": timed_calls(lambda: ref_mod.render(*args), a.calls),
+        "ours_dropin": timed_calls(lambda: F._C_stereo.render(*args), a.calls),
+        "images_identical": same,
+        "gpu": torch.cuda.get_device_name(),
+    }
+    res["speedup_median"] = res["reference_cuda"]["median_ms"] / res["ours_dropin"]["median_ms"]
+    print(json.dumps(res))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
