@@ -20,9 +20,8 @@ u16p = C.POINTER(C.c_uint16)
 u8p = C.POINTER(C.c_uint8)
 vp = C.c_void_p
 
-N_STAGES = 8
-STAGE_NAMES = ["setup_classify", "preprocess", "scan_create", "sort", "ranges", "blend_full", "blend_periphery",
-               "compose"]
+N_STAGES = 7
+STAGE_NAMES = ["setup_classify", "preprocess", "scan_create", "sort", "ranges_order", "blend", "compose"]
 
 STATUS = {
     0: "FHTGS_OK",

@@ -72,8 +72,8 @@ void set_last_error(const std::string& msg) { g_error = msg; }
 }  // namespace fhtgs
 
 // Stage boundaries recorded when profiling: start | setup+classify | preprocess |
-// scan+create | sort | ranges | blend full-res | blend periphery | compose.
-constexpr int kStageEvents = 9;
+// scan+create | sort | ranges+work order | blend | compose.
+constexpr int kStageEvents = FHTGS_N_STAGES + 1;
 constexpr int kStageRing = 64;   // frames whose stage events are kept
 
 struct fhtgs_context_s {
@@ -135,7 +135,7 @@ Layout plan(int V, int64_t N, int nbp, int64_t cap, int key_bytes, int sort_tile
     L.off_wm = take(4ull * V * max_large);
     L.off_ctr = take(4ull * kCounterWords);
     L.off_order0 = take(4ull * V * max_large);
-    L.off_order1 = take(4ull * V * max_large);
+    L.off_order1 = take(4);
     for (int64_t f : temp_floats) L.temp_offsets.push_back(f > 0 ? take(4ull * f) : 0);
     L.total = o;
     return L;
@@ -331,10 +331,10 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     n += ks.ranges(fp, fb, ctx->n_sms, stream);
     n += ks.order(fp, fb, ctx->n_sms, stream);
     mark(5);
-    n += ks.blend(fp, fb, ctx->n_sms, stream, prof ? ev[6] : nullptr);
-    mark(7);
+    n += ks.blend(fp, fb, ctx->n_sms, stream, nullptr);
+    mark(6);
     n += ks.compose(fp, fb, stream);
-    mark(8);
+    mark(7);
     FHTGS_CK(cudaGetLastError());
     ctx->launches += n;
     if (prof) ++ctx->frames_profiled;

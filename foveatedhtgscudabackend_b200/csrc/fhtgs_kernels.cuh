@@ -839,17 +839,24 @@ int launch_ranges(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cuda
 
 // ------------------------------------------------------------------------------------------
 // work ordering for the persistent blend (bucketed longest-processing-time first)
+// One list holds both kinds of tile: full-resolution (fovea + blended, 8 warps of pixels) and
+// periphery (8 x 8 samples at stride 2, 2 warps).  An item is packed as
+//   view << 24 | periphery << 23 | index into the view's work_full / work_low list.
+// Its cost is (warps x list length); items are bucketed by cost in quarter octaves and the
+// buckets are served heaviest first, so that long serial per-pixel chains start early.
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ int list_count(const FrameStatus& st, int list) {
-    return list == 0 ? static_cast<int>(st.n_fovea_large + st.n_blended_large) : static_cast<int>(st.n_periphery_large);
+constexpr uint32_t kItemLowres = 1u << 23;
+
+__device__ __forceinline__ int items_of_view(const FrameStatus& st) {
+    return static_cast<int>(st.n_fovea_large + st.n_blended_large + st.n_periphery_large);
 }
 
-__device__ __forceinline__ int cost_bucket(uint32_t len) {
-    return len == 0 ? 0 : min(kOrderBuckets - 1, 1 + __float2int_rd(4.0f * __log2f(static_cast<float>(len))));
+__device__ __forceinline__ int cost_bucket(uint32_t cost) {
+    return cost == 0 ? 0 : min(kOrderBuckets - 1, 1 + __float2int_rd(4.0f * __log2f(static_cast<float>(cost))));
 }
 
-// Maps flat item g of `list` to (view, item within the view); `pre` holds the exclusive prefix
-// of the per-view counts.
+// Maps flat item g to (view, index within the view); `pre` holds the exclusive prefix of the
+// per-view item counts.
 __device__ __forceinline__ void item_of(int g, const int* pre, int n_views, int& v, int& j) {
     int lo = 0, hi = n_views - 1;
     while (lo < hi) {
@@ -860,23 +867,31 @@ __device__ __forceinline__ void item_of(int g, const int* pre, int n_views, int&
     j = g - pre[lo];
 }
 
-__device__ __forceinline__ uint32_t item_len(const FrameParams& fp, const FrameBuffers& fb, int list, int v, int j) {
-    const uint32_t lt = list == 0 ? fb.work_full[static_cast<size_t>(v) * fp.max_large + j]
-                                  : fb.work_low[static_cast<size_t>(v) * fp.max_large + j];
+// Packed item and cost of the view's j-th item (full-resolution tiles first).
+__device__ __forceinline__ uint32_t item_cost(const FrameParams& fp, const FrameBuffers& fb, int v, int j,
+                                              uint32_t& packed) {
+    const FrameStatus& st = fb.status[v];
+    const int n_full = static_cast<int>(st.n_fovea_large + st.n_blended_large);
+    const bool low = j >= n_full;
+    const int idx = low ? j - n_full : j;
+    const uint32_t lt = low ? fb.work_low[static_cast<size_t>(v) * fp.max_large + idx]
+                            : fb.work_full[static_cast<size_t>(v) * fp.max_large + idx];
     const uint2 r = fb.ranges[static_cast<size_t>(v) * fp.max_large + lt];
-    return r.y > r.x ? r.y - r.x : 0u;
+    packed = (static_cast<uint32_t>(v) << 24) | (low ? kItemLowres : 0u) | static_cast<uint32_t>(idx);
+    const uint32_t len = r.y > r.x ? r.y - r.x : 0u;
+    return len * (low ? 2u : 8u);
 }
 
 constexpr int kMaxOrderViews = 1024;
 
-// Per-view prefix of the list counts into shared memory; returns the total.
-__device__ __forceinline__ int list_prefix(const FrameParams& fp, const FrameBuffers& fb, int list, int* pre) {
+// Per-view prefix of the item counts into shared memory; returns the total.
+__device__ __forceinline__ int items_prefix(const FrameParams& fp, const FrameBuffers& fb, int* pre) {
     __shared__ int s_total;
     if (threadIdx.x == 0) {
         int acc = 0;
         for (int v = 0; v < fp.n_views; ++v) {
             pre[v] = acc;
-            acc += list_count(fb.status[v], list);
+            acc += items_of_view(fb.status[v]);
         }
         s_total = acc;
     }
@@ -887,17 +902,17 @@ __device__ __forceinline__ int list_prefix(const FrameParams& fp, const FrameBuf
 __global__ void __launch_bounds__(256) order_hist_kernel(FrameParams fp, FrameBuffers fb) {
     __shared__ int pre[kMaxOrderViews];
     __shared__ uint32_t hist[kOrderBuckets];
-    const int list = blockIdx.y;
-    const int total = list_prefix(fp, fb, list, pre);
+    const int total = items_prefix(fp, fb, pre);
     for (int k = threadIdx.x; k < kOrderBuckets; k += blockDim.x) hist[k] = 0;
     __syncthreads();
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
         int v, j;
         item_of(g, pre, fp.n_views, v, j);
-        atomicAdd(&hist[cost_bucket(item_len(fp, fb, list, v, j))], 1u);
+        uint32_t packed;
+        atomicAdd(&hist[cost_bucket(item_cost(fp, fb, v, j, packed))], 1u);
     }
     __syncthreads();
-    uint32_t* gh = fb.counters + 4 + list * kOrderBuckets;
+    uint32_t* gh = fb.counters + 4;
     for (int k = threadIdx.x; k < kOrderBuckets; k += blockDim.x)
         if (hist[k]) atomicAdd(&gh[k], hist[k]);
 }
@@ -905,10 +920,9 @@ __global__ void __launch_bounds__(256) order_hist_kernel(FrameParams fp, FrameBu
 __global__ void __launch_bounds__(256) order_scatter_kernel(FrameParams fp, FrameBuffers fb) {
     __shared__ int pre[kMaxOrderViews];
     __shared__ uint32_t base[kOrderBuckets];
-    const int list = blockIdx.y;
-    const int total = list_prefix(fp, fb, list, pre);
-    const uint32_t* gh = fb.counters + 4 + list * kOrderBuckets;
-    uint32_t* cursor = fb.counters + 4 + 2 * kOrderBuckets + list * kOrderBuckets;
+    const int total = items_prefix(fp, fb, pre);
+    const uint32_t* gh = fb.counters + 4;
+    uint32_t* cursor = fb.counters + 4 + kOrderBuckets;
     if (threadIdx.x == 0) {  // descending bucket order
         uint32_t acc = 0;
         for (int k = kOrderBuckets - 1; k >= 0; --k) {
@@ -917,22 +931,22 @@ __global__ void __launch_bounds__(256) order_scatter_kernel(FrameParams fp, Fram
         }
     }
     __syncthreads();
-    uint32_t* out = fb.work_order[list];
+    uint32_t* out = fb.work_order[0];
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
         int v, j;
         item_of(g, pre, fp.n_views, v, j);
-        const int b = cost_bucket(item_len(fp, fb, list, v, j));
-        const uint32_t pos = base[b] + atomicAdd(&cursor[b], 1u);
-        out[pos] = (static_cast<uint32_t>(v) << 24) | static_cast<uint32_t>(j);
+        uint32_t packed;
+        const int b = cost_bucket(item_cost(fp, fb, v, j, packed));
+        out[base[b] + atomicAdd(&cursor[b], 1u)] = packed;
     }
 }
 
 int launch_order(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s) {
-    const int per_list = fp.n_views * fp.max_large;
-    int blocks = (per_list + 255) / 256;
+    const int per_view = fp.max_large;
+    int blocks = (fp.n_views * per_view + 255) / 256;
     blocks = blocks < 2 * n_sms ? (blocks > 0 ? blocks : 1) : 2 * n_sms;
-    order_hist_kernel<<<dim3(blocks, 2), 256, 0, s>>>(fp, fb);
-    order_scatter_kernel<<<dim3(blocks, 2), 256, 0, s>>>(fp, fb);
+    order_hist_kernel<<<blocks, 256, 0, s>>>(fp, fb);
+    order_scatter_kernel<<<blocks, 256, 0, s>>>(fp, fb);
     return 2;
 }
 
@@ -1103,46 +1117,51 @@ __device__ __forceinline__ bool conic_meets_rect(const Conic& q, float ax0, floa
 // 8-wide, 4-high block of samples.
 // Resident blocks per SM the register allocation has to allow: the K-buffer (2 K registers)
 // dominates for large K.
-__host__ __device__ constexpr int blend_min_blocks(int K, bool lowres) {
-    return lowres ? (K >= 32 ? 8 : K >= 16 ? 12 : 16) : (K >= 32 ? 2 : K >= 16 ? 3 : 4);
-}
+__host__ __device__ constexpr int blend_min_blocks(int K) { return K >= 32 ? 2 : K >= 16 ? 3 : 4; }
 
-template <int K, bool LOWRES>
-__global__ void __launch_bounds__(LOWRES ? 64 : 256, blend_min_blocks(K, LOWRES)) blend_kernel(FrameParams fp, FrameBuffers fb, int counter_idx) {
-    constexpr int NT = LOWRES ? 64 : 256;
+// One persistent kernel blends every tile of every view.  A block takes the next item of the
+// ordered work list and renders one 16x16 area: a full-resolution tile with its 8 warps (each
+// 8 x 4 pixels, laid out 2 x 4), or a periphery tile sampled at stride 2 with warps 0-1 (each
+// 8 x 4 samples, stacked), warps 2-7 idle.  The Gaussians of the tile's list are staged in
+// shared memory 256 at a time; each thread culls one of them against the 8 warp rectangles,
+// and every warp then walks only its own compacted list, in list order.
+template <int K>
+__global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FrameParams fp, FrameBuffers fb) {
+    constexpr int NT = 256;
     constexpr int NW = NT / 32;
-    constexpr int S = LOWRES ? kStride : 1;
     __shared__ float4 s_p1[NT], s_p2[NT], s_p4[NT], s_rgba[NT];
     __shared__ uint32_t s_mask[NT];
+    __shared__ uint8_t s_list[NW][NT];
     __shared__ int s_item;
-    // Warp w covers 8 x 4 samples: full resolution lays the 8 warps out 2 x 4 over the 16 x 16
-    // tile, the periphery grid (8 x 8 samples at stride 2) stacks its 2 warps vertically.
-    constexpr int WX = LOWRES ? 1 : 2;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int lx = (warp % WX) * 8 + (lane & 7);
-    const int ly = (warp / WX) * 4 + (lane >> 3);
-    // total work items over all views
+    const uint32_t lanemask_lt = (1u << lane) - 1u;
     int total = 0;
-    for (int v = 0; v < fp.n_views; ++v) total += list_count(fb.status[v], LOWRES ? 1 : 0);
-    const uint32_t* order = fb.work_order[LOWRES ? 1 : 0];
+    for (int v = 0; v < fp.n_views; ++v) total += items_of_view(fb.status[v]);
+    const uint32_t* order = fb.work_order[0];
     for (;;) {
-        if (tid == 0) s_item = static_cast<int>(atomicAdd(&fb.counters[counter_idx], 1u));
+        if (tid == 0) s_item = static_cast<int>(atomicAdd(&fb.counters[0], 1u));
         __syncthreads();
         const int g = s_item;
         __syncthreads();
         if (g >= total) break;
         const uint32_t packed = order[g];
         const int v = static_cast<int>(packed >> 24);
-        const int item = static_cast<int>(packed & 0xFFFFFFu);
+        const bool low = (packed & kItemLowres) != 0;
+        const int item = static_cast<int>(packed & (kItemLowres - 1u));
         const ViewParams& vp = fb.views[v];
         const FrameStatus& st = fb.status[v];
-        const uint32_t lt = LOWRES ? fb.work_low[static_cast<size_t>(v) * fp.max_large + item]
-                                   : fb.work_full[static_cast<size_t>(v) * fp.max_large + item];
-        const bool is_fovea = !LOWRES && static_cast<uint32_t>(item) < st.n_fovea_large;
+        const uint32_t lt = low ? fb.work_low[static_cast<size_t>(v) * fp.max_large + item]
+                                : fb.work_full[static_cast<size_t>(v) * fp.max_large + item];
+        const bool is_fovea = !low && static_cast<uint32_t>(item) < st.n_fovea_large;
+        const int S = low ? kStride : 1;
+        const int WX = low ? 1 : 2;
+        const int n_warps = low ? 2 : NW;
         const int ox = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)) * kTileLarge;
         const int oy = static_cast<int>(lt / static_cast<uint32_t>(vp.glw)) * kTileLarge;
+        const int lx = (warp % WX) * 8 + (lane & 7);
+        const int ly = (warp / WX) * 4 + (lane >> 3);
         const int px_i = ox + lx * S, py_i = oy + ly * S;
-        const bool inside = px_i < vp.width && py_i < vp.height;
+        const bool inside = warp < n_warps && px_i < vp.width && py_i < vp.height;
         const float pixel_x = __uint2float_rn(static_cast<uint32_t>(px_i));
         const float pixel_y = __uint2float_rn(static_cast<uint32_t>(py_i));
         const uint2 range = fb.ranges[static_cast<size_t>(v) * fp.max_large + lt];
@@ -1168,15 +1187,14 @@ __global__ void __launch_bounds__(LOWRES ? 64 : 256, blend_min_blocks(K, LOWRES)
                 s_rgba[tid] = c;
                 float4 box;
                 bool never;
-                uint32_t m = (1u << NW) - 1u;
+                uint32_t m = (1u << n_warps) - 1u;
                 if (cutoff_box(P1, P2, P4, c.w, box, never)) {
                     if (never) m = 0u;
                     else {
                         Conic q;
                         const bool ell = cutoff_conic(P1, P2, P4, c.w, q);
                         m = 0u;
-#pragma unroll
-                        for (int w = 0; w < NW; ++w) {
+                        for (int w = 0; w < n_warps; ++w) {
                             const float ax0 = static_cast<float>(ox + (w % WX) * 8 * S), ax1 = ax0 + 7.0f * S;
                             const float ay0 = static_cast<float>(oy + (w / WX) * 4 * S), ay1 = ay0 + 3.0f * S;
                             if (box.y >= ax0 && box.x <= ax1 && box.w >= ay0 && box.z <= ay1 &&
@@ -1188,9 +1206,19 @@ __global__ void __launch_bounds__(LOWRES ? 64 : 256, blend_min_blocks(K, LOWRES)
                 s_mask[tid] = m;
             }
             __syncthreads();
-            for (uint32_t j = 0; j < n_batch; ++j) {
-                if (!((s_mask[j] >> warp) & 1u)) continue;
-                if (!inside) continue;
+            // this warp's list: the batch positions whose mask has its bit, in order
+            int n_mine = 0;
+            for (uint32_t c0 = 0; c0 < n_batch; c0 += 32) {
+                const uint32_t j = c0 + lane;
+                const bool hit = j < n_batch && ((s_mask[j] >> warp) & 1u);
+                const uint32_t b = __ballot_sync(0xffffffffu, hit);
+                if (hit) s_list[warp][n_mine + __popc(b & lanemask_lt)] = static_cast<uint8_t>(j);
+                n_mine += __popc(b);
+            }
+            __syncwarp();
+            if (!inside) continue;
+            for (int t = 0; t < n_mine; ++t) {
+                const int j = s_list[warp][t];
                 const float4 VPMT1 = s_p1[j], VPMT2 = s_p2[j], VPMT4 = s_p4[j];
                 const float4 plane_x = VPMT1 - VPMT4 * pixel_x;
                 const float4 plane_y = VPMT2 - VPMT4 * pixel_y;
@@ -1215,9 +1243,9 @@ __global__ void __launch_bounds__(LOWRES ? 64 : 256, blend_min_blocks(K, LOWRES)
 #pragma unroll
                     for (int k = 0; k < K; ++k) {
                         if (f.depth < core[k].depth) {
-                            const Frag t = core[k];
+                            const Frag tf = core[k];
                             core[k] = f;
-                            f = t;
+                            f = tf;
                         }
                     }
                     pm = unpack_rgba(f.color);
@@ -1256,17 +1284,11 @@ __global__ void __launch_bounds__(LOWRES ? 64 : 256, blend_min_blocks(K, LOWRES)
 
 template <int K>
 int launch_blend_k(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid) {
-    static int occ_full = -1, occ_low = -1;  // per instantiation, queried once
-    if (occ_full < 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_full, blend_kernel<K, false>, 256, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_low, blend_kernel<K, true>, 64, 0);
-    }
-    const int gfull = n_sms * (occ_full > 0 ? occ_full : 1);
-    const int glow = n_sms * (occ_low > 0 ? occ_low : 1);
-    blend_kernel<K, false><<<gfull, 256, 0, s>>>(fp, fb, 0);
+    static int occ = -1;  // per instantiation, queried once
+    if (occ < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, blend_kernel<K>, 256, 0);
+    blend_kernel<K><<<n_sms * (occ > 0 ? occ : 1), 256, 0, s>>>(fp, fb);
     if (mid) cudaEventRecord(mid, s);
-    blend_kernel<K, true><<<glow, 64, 0, s>>>(fp, fb, 1);
-    return 2;
+    return 1;
 }
 
 int launch_blend(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid) {

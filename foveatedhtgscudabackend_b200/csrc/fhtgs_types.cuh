@@ -124,15 +124,14 @@ struct FrameBuffers {
     uint32_t* work_low;       // [V][max_large] periphery large tiles
     uint32_t* work_masked;    // [V][max_large] masked large tiles
     uint32_t* counters;       // [kCounterWords]: work counters, then the work-order buckets
-    uint32_t* work_order[2];  // [V*max_large] packed (view << 24 | item), heaviest first:
-                              // [0] fovea+blended tiles, [1] periphery tiles
+    uint32_t* work_order[2];  // [0]: [V*max_large] packed blend items, heaviest first; [1] unused
 };
 
 // Work ordering: tiles are bucketed by list length in quarter octaves and blended in
 // descending bucket order, so that the longest lists start first (longest-processing-time
 // scheduling of the persistent blend blocks).
 constexpr int kOrderBuckets = 130;
-constexpr int kCounterWords = 4 + 2 * 2 * kOrderBuckets;  // counters, histograms, cursors
+constexpr int kCounterWords = 4 + 2 * kOrderBuckets;  // counters, histogram, cursors
 
 // Launchers exported by each math flavour (fast = -use_fast_math, ieee = default).
 struct KernelSet {
@@ -145,7 +144,7 @@ struct KernelSet {
     int (*sort)(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s);
     int (*ranges)(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s);
     int (*order)(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s);
-    // `mid` (may be null) is recorded between the full-resolution and the periphery blend.
+    // `mid` (may be null) is recorded right after the blend.
     int (*blend)(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid);
     int (*compose)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);
 };

@@ -132,10 +132,10 @@ int64_t fhtgs_context_launch_count(fhtgs_context ctx);
 
 /* ---- stage timing ----
  * With profiling on, every frame records CUDA events on its stream between the stages:
- *   0 setup+classify, 1 preprocess, 2 scan+create instances, 3 sort, 4 tile ranges,
- *   5 blend full-resolution tiles, 6 blend periphery tiles, 7 compose.
+ *   0 setup+classify, 1 preprocess, 2 scan+create instances, 3 sort,
+ *   4 tile ranges + blend work order, 5 blend (all tiles), 6 compose.
  * fhtgs_get_stage_times waits for the last frame and returns the milliseconds per stage. */
-#define FHTGS_N_STAGES 8
+#define FHTGS_N_STAGES 7
 fhtgs_status fhtgs_context_set_profiling(fhtgs_context ctx, int32_t enable);
 fhtgs_status fhtgs_get_stage_times(fhtgs_context ctx, float* ms, int32_t n);
 /* Stage times of up to the last 64 profiled frames, oldest first: ms[f*FHTGS_N_STAGES + s]. */

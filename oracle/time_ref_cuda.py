@@ -64,11 +64,13 @@ def main(argv=None) -> int:
     theirs = ref_mod.render(*args)
     torch.cuda.synchronize()
     same = [bool(torch.equal(x, y)) for x, y in zip(mine, theirs)]
+    maxabs = [float((x - y).abs().max()) for x, y in zip(mine, theirs)]
+    psnr = [float(10 * torch.log10(1.0 / torch.clamp(((x - y).double() ** 2).mean(), min=1e-30))) for x, y in zip(mine, theirs)]
     res = {
         "workload": f"stereo {a.n} Gaussians SH3, 2x{a.width}x{a.height}, K={a.K}",
         "reference_cuda": timed_calls(lambda: ref_mod.render(*args), a.calls),
         "ours_dropin": timed_calls(lambda: F._C_stereo.render(*args), a.calls),
-        "images_identical": same,
+        "images_identical": same, "max_abs": maxabs, "psnr_db": psnr,
         "gpu": torch.cuda.get_device_name(),
     }
     res["speedup_median"] = res["reference_cuda"]["median_ms"] / res["ours_dropin"]["median_ms"]

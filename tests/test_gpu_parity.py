@@ -80,6 +80,18 @@ def test_intermediates_bit_exact_vs_golden(renderer, name):
 
 
 @pytest.mark.parametrize("name", golden_cases())
+def test_images_bit_identical_vs_golden(renderer, name):
+    """The blend keeps the reference's per-pixel arithmetic and order: images match bit for bit."""
+    case, data = load_golden(name)
+    g, views, bg = case_inputs(case)
+    imgs = renderer.render(*F.gaussians_to_torch(g), settings_for(case, views, bg), to_chw=case["to_chw"],
+                           blur_periphery=case["blur"], aaa_mode=case["aaa"], fast_math=case["module"] != "_C")
+    for i, im in enumerate(imgs):
+        a, b = im.cpu().numpy(), data[f"v{i}_image"]
+        assert np.array_equal(a, b), f"{name}/view{i}: {np.count_nonzero(a != b)} values differ, max {max_abs(a, b):.3g}"
+
+
+@pytest.mark.parametrize("name", golden_cases())
 def test_dropin_images_vs_golden(name):
     case, data = load_golden(name)
     g, views, bg = case_inputs(case)
