@@ -21,7 +21,6 @@ own stereo frames of a replicated scene (weak scaling, no collective on the data
 from __future__ import annotations
 
 import argparse
-import datetime
 import json
 import os
 import statistics
@@ -128,38 +127,21 @@ def workload(a, rank: int):
 
 
 def dist_setup(a):
-    import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from foveatedhtgscudabackend_b200 import dist as D
     if a.impl == "reference":
-        return world, rank, local  # rank 0 alone runs the host-core arm; no process group needed
-    if world > 1:
-        import torch.distributed as dist
-        backend = "nccl" if torch.cuda.is_available() else "gloo"
-        if backend == "nccl":
-            torch.cuda.set_device(local)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
-    elif torch.cuda.is_available():
-        torch.cuda.set_device(local)
-    return world, rank, local
+        return D.world()  # rank 0 alone runs the host-core arm; no process group needed
+    return D.init()
 
 
 def max_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else torch.device("cpu")
-    t = torch.tensor([x], dtype=torch.float64, device=dev)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from foveatedhtgscudabackend_b200 import dist as D
+    return D.max_over_ranks(x) if world > 1 else x
 
 
 def barrier(world: int):
+    from foveatedhtgscudabackend_b200 import dist as D
     if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+        D.barrier()
 
 
 def cpu_baseline(g, views, a, budget_s: float) -> dict:
@@ -348,8 +330,8 @@ def main(argv=None) -> int:
             print(json.dumps(line), flush=True)
     finally:
         if world > 1 and a.impl == "ours":
-            import torch.distributed as dist
-            dist.destroy_process_group()
+            from foveatedhtgscudabackend_b200 import dist as D
+            D.finalize()
     return 0
 
 
