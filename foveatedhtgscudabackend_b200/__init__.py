@@ -2,7 +2,7 @@
 
 Drop-in for the rasterization path of TrueKuehli/FoveatedHTGSCudaBackend: the same
 `FoveatedHTGSRasterizer` / `RasterizerSettings` surface and the same positional `_C`,
-`_C_benchmarking` and `_C_stereo` entry points, backed by libfhtgs.so (hand-written sm_100a
+`_C_benchmarking`, `_C_stereo` and `_C_visualization` entry points, backed by libfhtgs.so (hand-written sm_100a
 kernels behind the C ABI in include/fhtgs.h).
 """
 from .rasterization import (  # noqa: F401
@@ -16,7 +16,9 @@ from .rasterization import (  # noqa: F401
     _C_stereo,
 )
 from ._lib import FhtgsError  # noqa: F401
+from .display import FoveatedHTGSVisualizer, _C_visualization, build_tile_masks, pack_display  # noqa: F401
 from .torch_scene import gaussians_to_torch, settings_from_view  # noqa: F401
 
-__all__ = ["FoveatedHTGSRasterizer", "RasterizerSettings", "BackgroundModel", "Renderer", "FhtgsError",
-           "gaussians_to_torch", "settings_from_view"]
+__all__ = ["FoveatedHTGSRasterizer", "FoveatedHTGSVisualizer", "RasterizerSettings", "BackgroundModel",
+           "GazeVisualizationType", "Renderer", "FhtgsError", "gaussians_to_torch", "settings_from_view",
+           "build_tile_masks", "pack_display"]

@@ -97,6 +97,10 @@ SIGNATURES = {
     "fhtgs_benchmark_mono": (_MONO_ARGS, c_i32),
     "fhtgs_render_stereo": (_STEREO_ARGS, c_i32),
     "fhtgs_sort_instances_noalloc": ([vp, vp, vp, vp, C.c_int64, c_i32, c_i32, vp], c_i32),
+    "fhtgs_build_tile_masks": ([vp, c_i32, c_i32, vp, vp, vp, vp], c_i32),
+    "fhtgs_pack_display": ([C.POINTER(vp), c_i32, c_i32, c_i32, c_i32, c_i32, vp, vp], c_i32),
+    "fhtgs_visualize_gaze": ([vp, c_i32, c_i32, c_f, c_f, c_f, c_f, c_f, c_i32, c_i32, c_i32, vp], c_i32),
+    "fhtgs_visualize_tile_boundaries": ([vp, c_i32, c_i32, vp, c_f, c_f, c_i32, vp], c_i32),
 }
 
 _lock = threading.Lock()

@@ -6,6 +6,8 @@ Translation units:
   csrc/kernels_fast.cu  -use_fast_math  (arithmetic of the reference's _C_benchmarking / _C_stereo)
   csrc/kernels_ieee.cu  IEEE            (arithmetic of the reference's _C)
   csrc/fhtgs_host.cu    context, arena, orchestration, C ABI (include/fhtgs.h)
+  csrc/fhtgs_noalloc.cu the instance sort with a static working array
+  csrc/fhtgs_extras.cu  tile-mask builder, display packing, debug overlays
 The CUDA runtime is linked statically; the library has no torch dependency.
 """
 from __future__ import annotations
@@ -32,6 +34,7 @@ UNITS = [
     ("kernels_ieee.cu", []),
     ("fhtgs_host.cu", []),
     ("fhtgs_noalloc.cu", []),
+    ("fhtgs_extras.cu", []),
 ]
 HEADERS = ["fhtgs_types.cuh", "fhtgs_math.cuh", "fhtgs_kernels.cuh"]
 

@@ -231,6 +231,48 @@ fhtgs_status fhtgs_sort_instances_noalloc(const void* keys_in, const uint32_t* v
                                           void* keys_out, uint32_t* values_out, int64_t n,
                                           int32_t key_bytes, int32_t end_bit, void* stream);
 
+/* ---- tile masks on the device ----
+ * No counterpart in the reference, which takes the three mask tensors precomputed by the
+ * calling framework (torch_bindings/rasterization.py:22-43; read at
+ * rasterization/include/utils/kernel_utils.cuh:168-210).  Builds them on `stream` from one byte
+ * per 16x16 tile of a width x height view (row-major, grid ceil(width/16) x ceil(height/16);
+ * non-zero = visible; NULL = every tile visible):
+ *   visibility_mask            ceil(tiles/32) words, bit t%32 of word t/32 = tile t visible
+ *   visibility_mask_area_table (grid_w+1)*(grid_h+1) summed-area table, leading zero row/column
+ *   fovea_mask_area_table      49*49 table counting 3 extra sub-tiles per tile of the 48x48
+ *                              window around the gaze whose centre is inside the 24-tile circle
+ *                              (gaze-independent; NULL = skip).
+ * One launch, no allocation. */
+fhtgs_status fhtgs_build_tile_masks(const uint8_t* visible_tiles, int32_t width, int32_t height,
+                                    uint32_t* visibility_mask, uint32_t* visibility_mask_area_table,
+                                    uint32_t* fovea_mask_area_table, void* stream);
+
+/* ---- display-ready output ----
+ * No counterpart in the reference (its images are float32 RGB).  Packs n_views (1..8) float
+ * images of width x height (HWC, or CHW when to_chw) into one RGBA8 (BGRA8 when bgra) image of
+ * (n_views*width) x height, views side by side left to right (stereo: left | right), alpha 255.
+ * Each channel: clamp to [0,1] (NaN -> 0), then trunc(fma(c, 255, 0.5)).  `images` is a host
+ * array of device pointers; `out` is device memory of 4*n_views*width*height bytes. */
+fhtgs_status fhtgs_pack_display(const float* const* images, int32_t n_views, int32_t width, int32_t height,
+                                int32_t to_chw, int32_t bgra, uint8_t* out, void* stream);
+
+/* ---- debug overlays (replace _C_visualization, torch_bindings/bindings_visualization.cpp:8-9) ----
+ * fhtgs_visualize_gaze: visualization/src/visualization_api.cu:13-35 + visualization.cu:27-57.
+ *   Draws a marker of visualization_size pixels in (r,g,b) at the gaze (host floats, clamped to
+ *   the image) into the device image: type 0 circle, 2 cross, any other value < 256 a square.
+ * fhtgs_visualize_tile_boundaries: visualization_api.cu:37-64 + visualization.cu:60-236.
+ *   Outlines every visible tile of `visibility_mask` (device words as above) by its class for the
+ *   gaze: fovea sub-tiles orange (0.902,0.624,0), blended sub-tiles light blue
+ *   (0.337,0.706,0.914), periphery tiles green (0,0.620,0.451); nothing when at most one tile
+ *   entry is active, as in the reference.  One launch, no host synchronisation.
+ * Both asynchronous on `stream`; image is HWC float32 RGB, or CHW when to_chw. */
+fhtgs_status fhtgs_visualize_gaze(float* image, int32_t width, int32_t height, float gaze_x, float gaze_y,
+                                  float r, float g, float b, int32_t visualization_type,
+                                  int32_t visualization_size, int32_t to_chw, void* stream);
+fhtgs_status fhtgs_visualize_tile_boundaries(float* image, int32_t width, int32_t height,
+                                             const uint32_t* visibility_mask, float gaze_x, float gaze_y,
+                                             int32_t to_chw, void* stream);
+
 /* ---- errors / version ---- */
 const char* fhtgs_last_error(void);   /* thread-local message of the last failure */
 int32_t fhtgs_abi_version(void);

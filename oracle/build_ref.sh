@@ -10,9 +10,11 @@
 #                    + torch_utils.cpp, plus -O3 -use_fast_math               (setup.py:63-88)
 #   _C_stereo      = bindings_stereo.cpp + inference_stereo_api.cu + inference_stereo.cu
 #                    + torch_utils.cpp, plus -O3 -use_fast_math               (setup.py:63-99)
+#   _C_visualization = bindings_visualization.cpp + visualization_api.cu + visualization.cu
+#                    + torch_utils.cpp, plus -O3 -use_fast_math               (setup.py:32-50,101-110)
 # Only the architecture is added: -gencode arch=compute_100a,code=sm_100a.
 #
-# Usage: oracle/build_ref.sh [module ...]   (default: _C _C_benchmarking _C_stereo)
+# Usage: oracle/build_ref.sh [module ...]   (default: _C _C_benchmarking _C_stereo _C_visualization)
 set -euo pipefail
 REF=${REF_ROOT:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -59,13 +61,14 @@ build_module() {
   echo "built $OUT/$name$EXT"
 }
 
-MODS=("$@"); [ ${#MODS[@]} -eq 0 ] && MODS=(_C _C_benchmarking _C_stereo)
+MODS=("$@"); [ ${#MODS[@]} -eq 0 ] && MODS=(_C _C_benchmarking _C_stereo _C_visualization)
 RS="$FHB/rasterization/src"; TB="$FHB/torch_bindings"
 for m in "${MODS[@]}"; do
   case $m in
     _C) build_module _C 0 "$TB/bindings.cpp" "$RS/inference_api.cu" "$RS/inference.cu" "$RS/utils/torch_utils.cpp" ;;
     _C_benchmarking) build_module _C_benchmarking 1 "$TB/bindings_benchmarking.cpp" "$RS/fast_inference_api.cu" "$RS/inference.cu" "$RS/utils/torch_utils.cpp" ;;
     _C_stereo) build_module _C_stereo 1 "$TB/bindings_stereo.cpp" "$RS/inference_stereo_api.cu" "$RS/inference_stereo.cu" "$RS/utils/torch_utils.cpp" ;;
+    _C_visualization) build_module _C_visualization 1 "$TB/bindings_visualization.cpp" "$FHB/visualization/src/visualization_api.cu" "$FHB/visualization/src/visualization.cu" "$RS/utils/torch_utils.cpp" ;;
     *) echo "unknown module $m" >&2; exit 2 ;;
   esac
 done
