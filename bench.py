@@ -58,6 +58,9 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--cpu-budget-s", type=float, default=30.0, help="upper bound of the CPU baseline sample")
+    ap.add_argument("--workload", choices=["stereo", "batched"], default="stereo",
+                    help="stereo: the headline stereo frame; batched: 64 mixed-resolution cameras of a 3M scene")
+    ap.add_argument("--n-views", type=int, default=64, help="cameras per batch (batched workload)")
     return ap.parse_args(argv)
 
 
@@ -316,6 +319,87 @@ def run_ours(a, world, rank, local):
 
 
 # ------------------------------------------------------------------------------------------
+# batched workload: many cameras of uneven resolution and gaze per frame
+# ------------------------------------------------------------------------------------------
+def run_batched(a, world, rank, local):
+    """64 cameras on a sphere (r in [4, 8]) with resolutions drawn from {640x480, 1280x720,
+    1920x1080, 2064x2208} and random gaze, of one 3M-Gaussian SH3 scene, K = 8.  Three ways:
+    the batch as one captured frame graph after autotuning (`value`), the batch as one eager
+    frame, and the plain per-request path (each view through the blocking drop-in
+    `_C_benchmarking.benchmark`, one call per view)."""
+    import torch
+
+    import foveatedhtgscudabackend_b200 as F
+    from foveatedhtgscudabackend_b200 import _C_benchmarking, scene
+
+    dev = torch.device("cuda", local)
+    n_gauss = a.n_gaussians if a.n_gaussians != 1_000_000 else 3_000_000
+    g = scene.make_gaussians(n_gauss, a.sh_degree, seed=0)
+    views = scene.make_batched_views(a.n_views, seed=rank)
+    active = (a.sh_degree + 1) ** 2
+    gt = F.gaussians_to_torch(g, dev)
+    st = [F.settings_from_view(v, K=a.K, active_sh_bases=active, device=dev) for v in views]
+    pixels = sum(v.width * v.height for v in views)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn, steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        ev[0].record(stream)
+        for k in range(steps):
+            fn()
+            ev[k + 1].record(stream)
+        torch.cuda.synchronize(dev)
+        per = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+        return max_over_ranks(ev[0].elapsed_time(ev[steps]), world), per
+
+    r = F.Renderer(dev)
+    imgs = [torch.empty((3, v.height, v.width), device=dev) for v in views]
+    r.render(*gt, st, images=imgs, sync=True)
+    tuning = r.autotune(*gt, st, repeats=2)
+    graph = r.capture(*gt, st, images=imgs, capacity_headroom=1.1)
+    for _ in range(max(a.warmup, 0)):
+        graph.launch()
+    launches0 = r.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    graph_ms, graph_per = timed(graph.launch, a.steps)
+    clk = clocks.stop()
+    launches = r.launch_count() - launches0
+    overflow = any(r.frame_info(i)["overflow"] for i in range(len(st)))
+    eager_ms, _ = timed(lambda: r.render(*gt, st, images=imgs, sync=False), a.steps)
+    graph.close()
+    r.close()
+    # plain per-request path: one blocking drop-in call per view
+    plain_steps = max(1, min(a.steps, 3))
+    for s in st[:4]:
+        _C_benchmarking.benchmark(*gt, *s.as_tuple(), True, False, False)
+    plain_ms, _ = timed(lambda: [_C_benchmarking.benchmark(*gt, *s.as_tuple(), True, False, False) for s in st],
+                        plain_steps)
+    if rank != 0:
+        return None
+    nv = len(st)
+    lat = sorted(graph_per)
+    return {
+        "metric": "batched views/s (mixed-resolution cameras, one captured frame graph per batch)",
+        "value": round(world * a.steps * nv / (graph_ms / 1000.0), 2), "unit": "views/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(graph_ms / a.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"batched_{nv}views_{n_gauss // 1000}k_sh{a.sh_degree}_k{a.K}", "n_gaussians": n_gauss,
+                   "views": nv, "megapixels_per_batch": round(pixels / 1e6, 2),
+                   "resolutions": "uniform from 640x480, 1280x720, 1920x1080, 2064x2208",
+                   "cameras": "sphere r in [4, 8] looking at the origin, gaze uniform in [-0.8, 0.8]^2 NDC",
+                   "foveation": "reference constants (one fovea ring + blend band + 2x-down periphery)",
+                   "l2": "inputs larger than L2"},
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p99": round(float(np.percentile(lat, 99)), 3)},
+        "eager_batch_views_per_s": round(world * a.steps * nv / (eager_ms / 1000.0), 2),
+        "plain_per_view_views_per_s": round(world * plain_steps * nv / (plain_ms / 1000.0), 2),
+        "tuning": tuning, "overflow": overflow, "gpu_launches": int(launches), "clocks": clk,
+    }
+
+
+# ------------------------------------------------------------------------------------------
 # reference arm: the reference algorithm on the host cores
 # ------------------------------------------------------------------------------------------
 def run_reference(a, world, rank):
@@ -341,7 +425,12 @@ def main(argv=None) -> int:
     a = parse(argv)
     world, rank, local = dist_setup(a)
     try:
-        line = run_reference(a, world, rank) if a.impl == "reference" else run_ours(a, world, rank, local)
+        if a.impl == "reference":
+            line = run_reference(a, world, rank)
+        elif a.workload == "batched":
+            line = run_batched(a, world, rank, local)
+        else:
+            line = run_ours(a, world, rank, local)
         if line is not None:
             print(json.dumps(line), flush=True)
     finally:

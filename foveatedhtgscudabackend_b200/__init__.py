@@ -10,6 +10,7 @@ from .rasterization import (  # noqa: F401
     FoveatedHTGSRasterizer,
     GazeVisualizationType,
     RasterizerSettings,
+    FrameGraph,
     Renderer,
     _C,
     _C_benchmarking,

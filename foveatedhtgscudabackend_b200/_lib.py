@@ -70,6 +70,10 @@ class Intermediates(C.Structure):
                 ("values", u32p), ("instance_ranges", u32p)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("blend_warp_width", c_i32), ("blend_blocks_per_sm", c_i32), ("sort_items", c_i32)]
+
+
 # Exported symbols and their signatures (mirrors include/fhtgs.h).
 _MONO_ARGS = [vp, vp, vp, vp, vp, vp, vp, c_i32, c_i32, vp, vp, vp, vp, c_f, c_f, vp, vp, vp, vp, c_i32, c_i32,
               c_i32, c_i32, c_i32, c_i32, c_i32, c_f, c_f, c_f, c_f, c_f, c_f, c_f, c_i32, c_i32, c_i32, vp, vp]
@@ -97,6 +101,14 @@ SIGNATURES = {
     "fhtgs_benchmark_mono": (_MONO_ARGS, c_i32),
     "fhtgs_render_stereo": (_STEREO_ARGS, c_i32),
     "fhtgs_sort_instances_noalloc": ([vp, vp, vp, vp, C.c_int64, c_i32, c_i32, vp], c_i32),
+    "fhtgs_context_set_tuning": ([vp, C.POINTER(Tuning)], c_i32),
+    "fhtgs_context_get_tuning": ([vp, C.POINTER(Tuning)], c_i32),
+    "fhtgs_autotune": ([vp, C.POINTER(Primitives), C.POINTER(View), c_i32, C.POINTER(Settings), c_i32,
+                        C.POINTER(Tuning), C.POINTER(C.c_float), vp], c_i32),
+    "fhtgs_frame_graph_create": ([vp, C.POINTER(Primitives), C.POINTER(View), c_i32, C.POINTER(Settings), vp, c_f,
+                                  C.POINTER(vp), vp], c_i32),
+    "fhtgs_frame_graph_launch": ([vp, vp], c_i32),
+    "fhtgs_frame_graph_destroy": ([vp], c_i32),
     "fhtgs_build_tile_masks": ([vp, c_i32, c_i32, vp, vp, vp, vp], c_i32),
     "fhtgs_pack_display": ([C.POINTER(vp), c_i32, c_i32, c_i32, c_i32, c_i32, vp, vp], c_i32),
     "fhtgs_visualize_gaze": ([vp, c_i32, c_i32, c_f, c_f, c_f, c_f, c_f, c_i32, c_i32, c_i32, vp], c_i32),

@@ -81,6 +81,9 @@ struct fhtgs_context_s {
     int n_sms = 148;
     char* arena = nullptr;
     size_t arena_bytes = 0;
+    long long arena_generation = 0;   // bumped whenever the arena moves (captured graphs go stale)
+    bool capturing = false;           // a frame graph is being captured: no profiling events
+    fhtgs_tuning tuning{8, 0, kSortItems};
     int64_t cap = 0;              // instance slots per view
     FrameStatus* h_status = nullptr;  // pinned
     int h_status_n = 0;
@@ -158,6 +161,7 @@ fhtgs_status ensure_arena(fhtgs_context ctx, size_t bytes) {
                                                  cudaGetErrorString(e));
     }
     ctx->arena_bytes = want;
+    ++ctx->arena_generation;
     return FHTGS_OK;
 }
 
@@ -197,8 +201,15 @@ int64_t estimate_capacity(int64_t n_prims) {
     return (c + kSortTile - 1) / kSortTile * kSortTile;
 }
 
+int sort_tiles_for(int64_t cap, int sort_items) {
+    const int64_t tile = static_cast<int64_t>(kSortThreads) * sort_items;
+    return static_cast<int>((cap + tile - 1) / tile);
+}
+
+// Enqueues one frame on `stream` (no host synchronisation).  `gaze_dev` (null or [n_views][2]
+// floats in device memory) replaces the views' host gaze values at run time.
 fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views, int n_views,
-                         const fhtgs_settings* s, cudaStream_t stream) {
+                         const fhtgs_settings* s, cudaStream_t stream, const float* gaze_dev = nullptr) {
     fhtgs_status st = validate(prims, views, n_views, s);
     if (st != FHTGS_OK) return st;
     FHTGS_CK(cudaSetDevice(ctx->device));
@@ -216,7 +227,7 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     const int64_t cap = ctx->cap;
     const int key_u32 = max_large > 65536 ? 1 : 0;
     const int nbp = static_cast<int>((N + kPrimBlock - 1) / kPrimBlock);
-    const int sort_tiles = static_cast<int>((cap + kSortTile - 1) / kSortTile);
+    const int sort_tiles = sort_tiles_for(cap, ctx->tuning.sort_items);
     std::vector<int64_t> temp_floats(V, 0);
     if (s->blur_periphery)
         for (int i = 0; i < V; ++i) temp_floats[i] = 3ll * views[i].width * views[i].height;
@@ -247,6 +258,8 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     fp.max_tiles = max_tiles;
     fp.max_large = max_large;
     fp.n_blocks_prim = nbp;
+    fp.blend_rw = ctx->tuning.blend_warp_width;
+    fp.blend_blocks = ctx->tuning.blend_blocks_per_sm;
 
     FrameBuffers fb{};
     fb.views = reinterpret_cast<ViewParams*>(A + L.off_views);
@@ -264,6 +277,7 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     fb.sort_hist = reinterpret_cast<uint32_t*>(A + L.off_hist);
     fb.sort_digit_tot = reinterpret_cast<uint32_t*>(A + L.off_dtot);
     fb.sort_tiles = N > 0 ? sort_tiles : 0;
+    fb.sort_items = ctx->tuning.sort_items;
     fb.ranges = reinterpret_cast<uint2*>(A + L.off_ranges);
     fb.tile_map_part = reinterpret_cast<uint32_t*>(A + L.off_map);
     fb.tile_type_part = reinterpret_cast<uint8_t*>(A + L.off_type);
@@ -284,6 +298,7 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
         su.VPM = v.VPM;
         su.VPR_inv = v.VPR_inv;
         su.cam = v.cam_position;
+        su.gaze = gaze_dev ? gaze_dev + 2 * i : nullptr;
         ViewParams& p = su.p;
         std::memset(&p, 0, sizeof(p));
         p.gaze_px = make_float2(g.gaze_px, g.gaze_py);
@@ -308,7 +323,7 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     Gaussians gs{prims->positions, prims->scales, prims->rotations, prims->opacities, prims->sh_0, prims->sh_rest};
     const KernelSet& ks = s->fast_math ? kernels_fast() : kernels_ieee();
 
-    const bool prof = ctx->profile;
+    const bool prof = ctx->profile && !ctx->capturing;
     cudaEvent_t* ev = ctx->ev[ctx->frames_profiled % kStageRing];
     auto mark = [&](int i) {
         if (prof) cudaEventRecord(ev[i], stream);
@@ -430,7 +445,7 @@ fhtgs_status fhtgs_context_reserve(fhtgs_context ctx, int32_t n_primitives, int3
     const int nbp = (n_primitives + kPrimBlock - 1) / kPrimBlock;
     std::vector<int64_t> temp(n_views, 3ll * max_width * max_height);
     Layout L = plan(n_views, n_primitives, nbp, ctx->cap, end_bit_of(n_tiles + 1) > 16 ? 4 : 2,
-                    static_cast<int>((ctx->cap + kSortTile - 1) / kSortTile), n_tiles, n_large, temp);
+                    sort_tiles_for(ctx->cap, kSortItemsMin), n_tiles, n_large, temp);
     return ensure_arena(ctx, L.total);
 }
 
@@ -571,6 +586,216 @@ fhtgs_status fhtgs_copy_intermediates(fhtgs_context ctx, int32_t view, fhtgs_int
         if (out->values) out->values[pos] = 0xFFFFFFFFu;
     }
     if (out->instance_ranges && T) std::memcpy(out->instance_ranges, rr.data(), 8 * T);
+    return FHTGS_OK;
+}
+
+// ---- tuning, autotuner, frame graphs ----------------------------------------------------
+
+fhtgs_status fhtgs_context_set_tuning(fhtgs_context ctx, const fhtgs_tuning* t) {
+    if (!ctx || !t) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
+    if (t->blend_warp_width != 4 && t->blend_warp_width != 8 && t->blend_warp_width != 16)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "blend_warp_width must be 4, 8 or 16");
+    if (t->blend_blocks_per_sm < 0 || t->blend_blocks_per_sm > 8)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "blend_blocks_per_sm must be in [0, 8]");
+    if (t->sort_items != 8 && t->sort_items != 12 && t->sort_items != 16)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "sort_items must be 8, 12 or 16");
+    ctx->tuning = *t;
+    return FHTGS_OK;
+}
+
+fhtgs_status fhtgs_context_get_tuning(fhtgs_context ctx, fhtgs_tuning* t) {
+    if (!ctx || !t) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
+    *t = ctx->tuning;
+    return FHTGS_OK;
+}
+
+namespace {
+
+float median_of(std::vector<float> v) {
+    if (v.empty()) return 0.0f;
+    std::sort(v.begin(), v.end());
+    const size_t n = v.size();
+    return n % 2 ? v[n / 2] : 0.5f * (v[n / 2 - 1] + v[n / 2]);
+}
+
+// Renders `repeats` frames with tuning `t` after one warm-up frame; medians of one stage's time
+// and of the whole frame (CUDA events between the stages).
+fhtgs_status time_candidate(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views, int n_views,
+                            const fhtgs_settings* s, cudaStream_t stream, const fhtgs_tuning& t, int repeats, int stage,
+                            float* stage_ms, float* frame_ms) {
+    ctx->tuning = t;
+    for (int r = 0; r <= repeats; ++r) {
+        fhtgs_status st = render_impl(ctx, prims, views, n_views, s, stream);
+        if (st != FHTGS_OK) return st;
+    }
+    FHTGS_CK(cudaStreamSynchronize(stream));
+    std::vector<float> st_ms, fr_ms;
+    for (int f = 0; f < repeats; ++f) {
+        cudaEvent_t* ev = ctx->ev[(ctx->frames_profiled - repeats + f) % kStageRing];
+        float a = 0.0f, b = 0.0f;
+        FHTGS_CK(cudaEventElapsedTime(&a, ev[stage], ev[stage + 1]));
+        FHTGS_CK(cudaEventElapsedTime(&b, ev[0], ev[kStageEvents - 1]));
+        st_ms.push_back(a);
+        fr_ms.push_back(b);
+    }
+    *stage_ms = median_of(st_ms);
+    *frame_ms = median_of(fr_ms);
+    return FHTGS_OK;
+}
+
+}  // namespace
+
+fhtgs_status fhtgs_autotune(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views, int32_t n_views,
+                            const fhtgs_settings* settings, int32_t repeats, fhtgs_tuning* best, float* best_frame_ms,
+                            void* stream_) {
+    if (!ctx || !best) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
+    if (repeats < 1 || repeats > 32) return fail(FHTGS_ERR_INVALID_ARGUMENT, "repeats must be in [1, 32]");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    const bool was_profiling = ctx->profile;
+    fhtgs_status st = fhtgs_context_set_profiling(ctx, 1);
+    if (st != FHTGS_OK) return st;
+    const fhtgs_tuning start = ctx->tuning;
+    auto finish = [&](fhtgs_status r) {
+        ctx->profile = was_profiling;
+        if (r != FHTGS_OK) ctx->tuning = start;
+        return r;
+    };
+    st = render_sync_impl(ctx, prims, views, n_views, settings, stream);  // sizes the capacity
+    if (st != FHTGS_OK) return finish(st);
+    constexpr int kStageSort = 3, kStageBlend = 5;
+    fhtgs_tuning cur = start;
+    float best_stage = 3.4e38f, frame = 0.0f, stage = 0.0f;
+    // blend: warp rectangle x persistent blocks per SM
+    fhtgs_tuning win = cur;
+    for (int w : kBlendRowChoices) {
+        for (int b : {0, 3, 2}) {
+            fhtgs_tuning t = cur;
+            t.blend_warp_width = w;
+            t.blend_blocks_per_sm = b;
+            st = time_candidate(ctx, prims, views, n_views, settings, stream, t, repeats, kStageBlend, &stage, &frame);
+            if (st != FHTGS_OK) return finish(st);
+            if (stage < best_stage) { best_stage = stage; win = t; }
+        }
+    }
+    cur = win;
+    // sort: keys per thread of a tile
+    best_stage = 3.4e38f;
+    for (int items : {16, 12, 8}) {
+        fhtgs_tuning t = cur;
+        t.sort_items = items;
+        st = time_candidate(ctx, prims, views, n_views, settings, stream, t, repeats, kStageSort, &stage, &frame);
+        if (st != FHTGS_OK) return finish(st);
+        if (stage < best_stage) { best_stage = stage; win = t; }
+    }
+    cur = win;
+    st = time_candidate(ctx, prims, views, n_views, settings, stream, cur, repeats, kStageBlend, &stage, &frame);
+    if (st != FHTGS_OK) return finish(st);
+    ctx->tuning = cur;
+    *best = cur;
+    if (best_frame_ms) *best_frame_ms = frame;
+    return finish(FHTGS_OK);
+}
+
+struct fhtgs_frame_graph_s {
+    fhtgs_context ctx = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long generation = 0;
+    long long launches_per_frame = 0;
+    FrameParams fp{};
+    FrameBuffers fb{};
+    std::vector<ViewGeom> geo;
+    std::vector<fhtgs_view> views;
+};
+
+fhtgs_status fhtgs_frame_graph_create(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views,
+                                      int32_t n_views, const fhtgs_settings* settings, const float* gaze_device,
+                                      float capacity_headroom, fhtgs_frame_graph* out, void* stream_) {
+    if (!ctx || !out) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (!(capacity_headroom >= 1.0f) || capacity_headroom > 16.0f)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "capacity_headroom must be in [1, 16]");
+    fhtgs_status st = validate(prims, views, n_views, settings);
+    if (st != FHTGS_OK) return st;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    // 1) an eager frame measures the instance counts; the capacity gets the headroom
+    st = render_sync_impl(ctx, prims, views, n_views, settings, stream);
+    if (st != FHTGS_OK) return st;
+    unsigned long long need = 0;
+    for (int i = 0; i < n_views; ++i) need = std::max(need, ctx->h_status[i].n_instances);
+    const int64_t want = static_cast<int64_t>(static_cast<double>(need) * capacity_headroom) + kSortTile;
+    if (want > ctx->cap) ctx->cap = (want + kSortTile - 1) / kSortTile * kSortTile;
+    // 2) a frame at the final capacity places the arena (nothing may allocate while capturing)
+    st = render_impl(ctx, prims, views, n_views, settings, stream, gaze_device);
+    if (st != FHTGS_OK) return st;
+    FHTGS_CK(cudaStreamSynchronize(stream));
+    // 3) capture the same frame on a private stream
+    cudaStream_t cs = nullptr;
+    FHTGS_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    const long long launches0 = ctx->launches;
+    const long long generation = ctx->arena_generation;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        ctx->capturing = true;
+        st = render_impl(ctx, prims, views, n_views, settings, cs, gaze_device);
+        ctx->capturing = false;
+        e = cudaStreamEndCapture(cs, &graph);
+    }
+    cudaStreamDestroy(cs);
+    ctx->stream = stream;  // the capture stream is gone; inspection reads follow the caller's
+    const long long per_frame = ctx->launches - launches0;
+    ctx->launches = launches0;
+    if (st != FHTGS_OK || e != cudaSuccess || ctx->arena_generation != generation) {
+        if (graph) cudaGraphDestroy(graph);
+        if (st != FHTGS_OK) return st;
+        if (e != cudaSuccess) return fail(FHTGS_ERR_CUDA, std::string("frame capture: ") + cudaGetErrorString(e));
+        return fail(FHTGS_ERR_CUDA, "the arena moved during the capture");
+    }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(FHTGS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    auto* g = new fhtgs_frame_graph_s();
+    g->ctx = ctx;
+    g->graph = graph;
+    g->exec = exec;
+    g->generation = generation;
+    g->launches_per_frame = per_frame;
+    g->fp = ctx->fp;
+    g->fb = ctx->fb;
+    g->geo = ctx->geo;
+    g->views = ctx->views;
+    *out = g;
+    return FHTGS_OK;
+}
+
+fhtgs_status fhtgs_frame_graph_launch(fhtgs_frame_graph g, void* stream_) {
+    if (!g) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null graph");
+    fhtgs_context ctx = g->ctx;
+    if (ctx->arena_generation != g->generation)
+        return fail(FHTGS_ERR_NOT_READY, "the context's arena moved since the capture; create the graph again");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    FHTGS_CK(cudaSetDevice(ctx->device));
+    FHTGS_CK(cudaGraphLaunch(g->exec, stream));
+    ctx->have_frame = true;
+    ctx->fp = g->fp;
+    ctx->fb = g->fb;
+    ctx->geo = g->geo;
+    ctx->views = g->views;
+    ctx->stream = stream;
+    ctx->launches += g->launches_per_frame;
+    return FHTGS_OK;
+}
+
+fhtgs_status fhtgs_frame_graph_destroy(fhtgs_frame_graph g) {
+    if (!g) return FHTGS_OK;
+    cudaSetDevice(g->ctx->device);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
     return FHTGS_OK;
 }
 

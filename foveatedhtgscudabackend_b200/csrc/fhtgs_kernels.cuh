@@ -80,16 +80,33 @@ __device__ __forceinline__ float4 ld4(const float* p) { return make_float4(p[0],
 // ------------------------------------------------------------------------------------------
 // setup
 // ------------------------------------------------------------------------------------------
-constexpr int kSetupChunk = 8;
+constexpr int kSetupChunk = 32;
 struct SetupChunk {
     ViewSetup v[kSetupChunk];
     int n, first;
 };
 
-__global__ void setup_kernel(SetupChunk c, ViewParams* __restrict__ out) {
+// Gaze clamp and rounding of the host path (fhtgs_host.cu: geometry(), after inference.cu:79-105
+// of the reference), for a gaze read from device memory: std::max/std::min as comparisons.
+__device__ __forceinline__ void gaze_from_device(ViewParams& p, const float* g) {
+    const float wm1 = static_cast<float>(p.width - 1), hm1 = static_cast<float>(p.height - 1);
+    float gx = g[0] < 0.0f ? 0.0f : g[0];
+    float gy = g[1] < 0.0f ? 0.0f : g[1];
+    gx = wm1 < gx ? wm1 : gx;
+    gy = hm1 < gy ? hm1 : gy;
+    const int gw = p.glw * kStride, gh = p.glh * kStride;
+    const int tx = max(0, min(gw - 1, (static_cast<int>(gx) + kTileLarge / 2) / kTileLarge));
+    const int ty = max(0, min(gh - 1, (static_cast<int>(gy) + kTileLarge / 2) / kTileLarge));
+    p.gaze_px = make_float2(gx, gy);
+    p.gaze_tiles = make_float2(static_cast<float>(tx), static_cast<float>(ty));
+    p.gaze_tiles_i = make_int2(tx, ty);
+}
+
+__global__ void setup_kernel(const __grid_constant__ SetupChunk c, ViewParams* __restrict__ out) {
     const int i = threadIdx.x;
     if (i >= c.n) return;
     ViewParams p = c.v[i].p;
+    if (c.v[i].gaze) gaze_from_device(p, c.v[i].gaze);
     for (int r = 0; r < 3; ++r) p.M[r] = ld4(c.v[i].M + 4 * r);
     for (int r = 0; r < 4; ++r) p.VPM[r] = ld4(c.v[i].VPM + 4 * r);
     for (int r = 0; r < 4; ++r) p.VPR_inv[r] = ld4(c.v[i].VPR_inv + 4 * r);
@@ -104,7 +121,7 @@ int launch_setup(const ViewSetup* setups, int n_views, ViewParams* out, cudaStre
         c.n = n_views - first < kSetupChunk ? n_views - first : kSetupChunk;
         c.first = first;
         for (int i = 0; i < c.n; ++i) c.v[i] = setups[first + i];
-        setup_kernel<<<1, 32, 0, s>>>(c, out);
+        setup_kernel<<<1, kSetupChunk, 0, s>>>(c, out);
         ++n;
     }
     return n;
@@ -649,21 +666,22 @@ __device__ __forceinline__ uint64_t view_count(const FrameParams& fp, const Fram
     return m < static_cast<unsigned long long>(fp.cap) ? m : static_cast<unsigned long long>(fp.cap);
 }
 
-template <typename KeyT>
+template <typename KeyT, int ITEMS>
 __global__ void __launch_bounds__(kSortThreads) sort_upsweep_kernel(FrameParams fp, FrameBuffers fb, int buf, int shift) {
+    constexpr int TILE = kSortThreads * ITEMS;
     __shared__ uint32_t s_hist[kSortThreads / 32][kSortBins];
     const int v = blockIdx.y;
     const uint64_t M = view_count(fp, fb, v);
-    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kSortTile;
+    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * TILE;
     if (t0 >= M) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int k = threadIdx.x; k < (kSortThreads / 32) * kSortBins; k += kSortThreads) (&s_hist[0][0])[k] = 0;
     __syncthreads();
-    const uint32_t n_here = static_cast<uint32_t>(M - t0 < static_cast<uint64_t>(kSortTile) ? M - t0 : kSortTile);
+    const uint32_t n_here = static_cast<uint32_t>(M - t0 < static_cast<uint64_t>(TILE) ? M - t0 : TILE);
     const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[buf]) + static_cast<size_t>(v) * fp.cap + t0;
-    const uint32_t wbase = static_cast<uint32_t>(warp) * 32 * kSortItems + lane;
+    const uint32_t wbase = static_cast<uint32_t>(warp) * 32 * ITEMS + lane;
 #pragma unroll 4
-    for (int it = 0; it < kSortItems; ++it) {
+    for (int it = 0; it < ITEMS; ++it) {
         const uint32_t idx = wbase + it * 32;
         const bool ok = idx < n_here;
         const uint32_t d = ok ? (static_cast<uint32_t>(keys[idx]) >> shift) & (kSortBins - 1) : kSortBins;
@@ -683,7 +701,8 @@ __global__ void __launch_bounds__(256) sort_scan_kernel(FrameParams fp, FrameBuf
     __shared__ uint32_t s_warp[33];
     const int d = blockIdx.x, v = blockIdx.y;
     const uint64_t M = view_count(fp, fb, v);
-    const int ntiles = static_cast<int>((M + kSortTile - 1) / kSortTile);
+    const int tile = kSortThreads * fb.sort_items;
+    const int ntiles = static_cast<int>((M + tile - 1) / tile);
     uint32_t* row = fb.sort_hist + (static_cast<size_t>(v) * kSortBins + d) * fb.sort_tiles;
     uint32_t carry = 0;
     for (int base = 0; base < ntiles; base += blockDim.x) {
@@ -697,34 +716,35 @@ __global__ void __launch_bounds__(256) sort_scan_kernel(FrameParams fp, FrameBuf
     if (threadIdx.x == 0) fb.sort_digit_tot[static_cast<size_t>(v) * kSortBins + d] = carry;
 }
 
-template <typename KeyT>
+template <typename KeyT, int ITEMS>
 __global__ void __launch_bounds__(kSortThreads, 3) sort_scatter_kernel(FrameParams fp, FrameBuffers fb, int buf, int shift) {
+    constexpr int TILE = kSortThreads * ITEMS;
     __shared__ uint32_t s_whist[kSortThreads / 32][kSortBins];  // per-warp counts, then running slots
     __shared__ uint32_t s_local_start[kSortBins];
     __shared__ uint32_t s_global_start[kSortBins];
     __shared__ uint32_t s_warp[33];
-    __shared__ KeyT s_keys[kSortTile];
-    __shared__ uint32_t s_vals[kSortTile];
+    __shared__ KeyT s_keys[TILE];
+    __shared__ uint32_t s_vals[TILE];
     const int v = blockIdx.y;
     const uint64_t M = view_count(fp, fb, v);
-    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kSortTile;
+    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * TILE;
     if (t0 >= M) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lanemask_lt = (1u << lane) - 1u;
     for (int k = threadIdx.x; k < (kSortThreads / 32) * kSortBins; k += kSortThreads) (&s_whist[0][0])[k] = 0;
     __syncthreads();
-    const uint32_t n_here = static_cast<uint32_t>(M - t0 < static_cast<uint64_t>(kSortTile) ? M - t0 : kSortTile);
+    const uint32_t n_here = static_cast<uint32_t>(M - t0 < static_cast<uint64_t>(TILE) ? M - t0 : TILE);
     const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[buf]) + static_cast<size_t>(v) * fp.cap + t0;
     const uint32_t* vals = fb.vals[buf] + static_cast<size_t>(v) * fp.cap + t0;
     KeyT* okeys = reinterpret_cast<KeyT*>(fb.keys[buf ^ 1]) + static_cast<size_t>(v) * fp.cap;
     uint32_t* ovals = fb.vals[buf ^ 1] + static_cast<size_t>(v) * fp.cap;
-    // Each warp owns 32 * kSortItems consecutive keys, visited warp-striped (coalesced loads);
+    // Each warp owns 32 * ITEMS consecutive keys, visited warp-striped (coalesced loads);
     // the visit order is the key order, which makes the ranking stable.
-    const uint32_t wbase = static_cast<uint32_t>(warp) * 32 * kSortItems + lane;
-    KeyT k_reg[kSortItems];
-    uint32_t v_reg[kSortItems];
+    const uint32_t wbase = static_cast<uint32_t>(warp) * 32 * ITEMS + lane;
+    KeyT k_reg[ITEMS];
+    uint32_t v_reg[ITEMS];
 #pragma unroll
-    for (int it = 0; it < kSortItems; ++it) {
+    for (int it = 0; it < ITEMS; ++it) {
         const uint32_t idx = wbase + it * 32;
         const bool ok = idx < n_here;
         k_reg[it] = ok ? keys[idx] : static_cast<KeyT>(0);
@@ -755,7 +775,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_scatter_kernel(FramePara
     __syncthreads();
     // second visit: stable slot of every key inside the tile
 #pragma unroll
-    for (int it = 0; it < kSortItems; ++it) {
+    for (int it = 0; it < ITEMS; ++it) {
         const bool ok = wbase + it * 32 < n_here;
         const uint32_t dd = ok ? (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1) : kSortBins;
         const uint32_t peers = __match_any_sync(0xffffffffu, dd);
@@ -779,25 +799,35 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_scatter_kernel(FramePara
     }
 }
 
-template <typename KeyT>
+// fb.sort_tiles must be ceil(cap / (kSortThreads * ITEMS)).
+template <typename KeyT, int ITEMS>
 int sort_t(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s) {
     const int passes = (fp.end_bit + kSortRadixBits - 1) / kSortRadixBits;
     int buf = 0;
     dim3 gt(fb.sort_tiles, fp.n_views), gd(kSortBins, fp.n_views);
     for (int p = 0; p < passes; ++p) {
         const int shift = p * kSortRadixBits;
-        sort_upsweep_kernel<KeyT><<<gt, kSortThreads, 0, s>>>(fp, fb, buf, shift);
+        sort_upsweep_kernel<KeyT, ITEMS><<<gt, kSortThreads, 0, s>>>(fp, fb, buf, shift);
         sort_scan_kernel<<<gd, 256, 0, s>>>(fp, fb);
-        sort_scatter_kernel<KeyT><<<gt, kSortThreads, 0, s>>>(fp, fb, buf, shift);
+        sort_scatter_kernel<KeyT, ITEMS><<<gt, kSortThreads, 0, s>>>(fp, fb, buf, shift);
         buf ^= 1;
     }
     fb.final_buf = buf;
     return 3 * passes;
 }
 
+template <typename KeyT>
+int sort_items_t(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s) {
+    switch (fb.sort_items) {
+        case 8: return sort_t<KeyT, 8>(fp, fb, s);
+        case 12: return sort_t<KeyT, 12>(fp, fb, s);
+        default: return sort_t<KeyT, 16>(fp, fb, s);
+    }
+}
+
 int launch_sort(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s) {
     if (fb.sort_tiles == 0) { fb.final_buf = 0; return 0; }
-    return fp.key_u32 ? sort_t<uint32_t>(fp, fb, s) : sort_t<uint16_t>(fp, fb, s);
+    return fp.key_u32 ? sort_items_t<uint32_t>(fp, fb, s) : sort_items_t<uint16_t>(fp, fb, s);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1121,11 +1151,13 @@ __host__ __device__ constexpr int blend_min_blocks(int K) { return K >= 32 ? 2 :
 
 // One persistent kernel blends every tile of every view.  A block takes the next item of the
 // ordered work list and renders one 16x16 area: a full-resolution tile with its 8 warps (each
-// 8 x 4 pixels, laid out 2 x 4), or a periphery tile sampled at stride 2 with warps 0-1 (each
-// 8 x 4 samples, stacked), warps 2-7 idle.  The Gaussians of the tile's list are staged in
-// shared memory 256 at a time; each thread culls one of them against the 8 warp rectangles,
-// and every warp then walks only its own compacted list, in list order.
-template <int K>
+// RW x 32/RW pixels: 8 x 4 laid out 2 x 4, 16 x 2 stacked, or 4 x 8 laid out 4 x 2), or a
+// periphery tile sampled at stride 2 with warps 0-1 (each min(RW, 8) wide), warps 2-7 idle.
+// The Gaussians of the tile's list are staged in shared memory 256 at a time; each thread
+// culls one of them against the warp rectangles, and every warp then walks only its own
+// compacted list, in list order.  The warp shape only changes which pairs are culled (pairs
+// that cannot pass the alpha test), never a pixel's arithmetic.
+template <int K, int RW>
 __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FrameParams fp, FrameBuffers fb) {
     constexpr int NT = 256;
     constexpr int NW = NT / 32;
@@ -1154,12 +1186,17 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
                                 : fb.work_full[static_cast<size_t>(v) * fp.max_large + item];
         const bool is_fovea = !low && static_cast<uint32_t>(item) < st.n_fovea_large;
         const int S = low ? kStride : 1;
-        const int WX = low ? 1 : 2;
+        // warp rectangle rw x rh (powers of two); warps laid out 2^wx_bits per row
+        constexpr int RW_LOW = RW > 8 ? 8 : RW;  // the periphery sample grid is 8 wide
+        constexpr int RW_BITS = RW == 4 ? 2 : RW == 8 ? 3 : 4, RW_LOW_BITS = RW_LOW == 4 ? 2 : 3;
+        const int rw_bits = low ? RW_LOW_BITS : RW_BITS;
+        const int rw = 1 << rw_bits, rh = 32 >> rw_bits;
+        const int wx_bits = (low ? 3 : 4) - rw_bits;
         const int n_warps = low ? 2 : NW;
         const int ox = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)) * kTileLarge;
         const int oy = static_cast<int>(lt / static_cast<uint32_t>(vp.glw)) * kTileLarge;
-        const int lx = (warp % WX) * 8 + (lane & 7);
-        const int ly = (warp / WX) * 4 + (lane >> 3);
+        const int lx = (warp & ((1 << wx_bits) - 1)) * rw + (lane & (rw - 1));
+        const int ly = (warp >> wx_bits) * rh + (lane >> rw_bits);
         const int px_i = ox + lx * S, py_i = oy + ly * S;
         const bool inside = warp < n_warps && px_i < vp.width && py_i < vp.height;
         const float pixel_x = __uint2float_rn(static_cast<uint32_t>(px_i));
@@ -1195,8 +1232,10 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
                         const bool ell = cutoff_conic(P1, P2, P4, c.w, q);
                         m = 0u;
                         for (int w = 0; w < n_warps; ++w) {
-                            const float ax0 = static_cast<float>(ox + (w % WX) * 8 * S), ax1 = ax0 + 7.0f * S;
-                            const float ay0 = static_cast<float>(oy + (w / WX) * 4 * S), ay1 = ay0 + 3.0f * S;
+                            const float ax0 = static_cast<float>(ox + (w & ((1 << wx_bits) - 1)) * rw * S);
+                            const float ax1 = ax0 + static_cast<float>((rw - 1) * S);
+                            const float ay0 = static_cast<float>(oy + (w >> wx_bits) * rh * S);
+                            const float ay1 = ay0 + static_cast<float>((rh - 1) * S);
                             if (box.y >= ax0 && box.x <= ax1 && box.w >= ay0 && box.z <= ay1 &&
                                 (!ell || conic_meets_rect(q, ax0, ax1, ay0, ay1)))
                                 m |= 1u << w;
@@ -1282,13 +1321,24 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
     }
 }
 
-template <int K>
-int launch_blend_k(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid) {
+template <int K, int RW>
+int launch_blend_kr(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid) {
     static int occ = -1;  // per instantiation, queried once
-    if (occ < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, blend_kernel<K>, 256, 0);
-    blend_kernel<K><<<n_sms * (occ > 0 ? occ : 1), 256, 0, s>>>(fp, fb);
+    if (occ < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, blend_kernel<K, RW>, 256, 0);
+    int per_sm = occ > 0 ? occ : 1;
+    if (fp.blend_blocks > 0 && fp.blend_blocks < per_sm) per_sm = fp.blend_blocks;
+    blend_kernel<K, RW><<<n_sms * per_sm, 256, 0, s>>>(fp, fb);
     if (mid) cudaEventRecord(mid, s);
     return 1;
+}
+
+template <int K>
+int launch_blend_k(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid) {
+    switch (fp.blend_rw) {
+        case 16: return launch_blend_kr<K, 16>(fp, fb, n_sms, s, mid);
+        case 4: return launch_blend_kr<K, 4>(fp, fb, n_sms, s, mid);
+        default: return launch_blend_kr<K, 8>(fp, fb, n_sms, s, mid);
+    }
 }
 
 int launch_blend(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid) {

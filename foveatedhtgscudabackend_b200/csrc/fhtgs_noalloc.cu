@@ -109,6 +109,7 @@ extern "C" fhtgs_status fhtgs_sort_instances_noalloc(const void* keys_in, const 
     fb.sort_digit_tot = reinterpret_cast<uint32_t*>(scratch + kOffDigitTot);
     fb.sort_hist = reinterpret_cast<uint32_t*>(scratch + kOffHist);
     fb.sort_tiles = static_cast<int>((n + fhtgs::kSortTile - 1) / fhtgs::kSortTile);
+    fb.sort_items = fhtgs::kSortItems;
     // Ping-pong between the caller's output and the scratch buffer; the input stays untouched.
     fb.keys[0] = keys_out;
     fb.vals[0] = values_out;

@@ -54,6 +54,7 @@ struct ViewSetup {
     const float* VPM;
     const float* VPR_inv;
     const float* cam;
+    const float* gaze;     // device (x, y) read by the setup kernel, or null: gaze fields of p are used
     ViewParams p;          // scalars filled on the host, matrices gathered on the device
 };
 
@@ -75,6 +76,8 @@ struct FrameParams {
     int max_tiles;         // max small-tile ids over views (stride of per-tile arrays)
     int max_large;         // max large tiles over views
     int n_blocks_prim;     // preprocess/create blocks per view
+    int blend_rw;          // blend: pixels per warp row (4, 8 or 16; 32 / blend_rw rows)
+    int blend_blocks;      // persistent blend blocks per SM (0: as many as fit)
 };
 
 // Per-view frame status written by the device, read by the host after the frame.
@@ -116,6 +119,7 @@ struct FrameBuffers {
     uint32_t* sort_hist;      // [V][256][sort_tiles]
     uint32_t* sort_digit_tot; // [V][256]
     int sort_tiles;           // tiles of the radix sort per view (capacity based)
+    int sort_items;           // keys per thread of a sort tile (kSortItemChoices)
     uint2* ranges;            // [V][max_large] instance range per large tile
     uint32_t* tile_map_part;  // [V][max_tiles]
     uint8_t* tile_type_part;  // [V][max_tiles]
@@ -154,8 +158,11 @@ const KernelSet& kernels_ieee();
 
 constexpr int kPrimBlock = 256;      // preprocess / create-instances block
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;        // keys per thread per sort tile
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
+constexpr int kSortItems = 16;        // default keys per thread per sort tile
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 (default tile)
+constexpr int kSortItemsMin = 8;      // smallest tile the autotuner may choose (2048 keys)
+// Blend warp rectangles the autotuner may choose: pixels per warp row.
+constexpr int kBlendRowChoices[3] = {8, 16, 4};
 constexpr int kSortRadixBits = 8;
 constexpr int kSortBins = 1 << kSortRadixBits;
 

@@ -326,10 +326,9 @@ class Renderer:
         return [dict(zip(_lib.STAGE_NAMES, [float(x) for x in buf[f * _lib.N_STAGES:(f + 1) * _lib.N_STAGES]]))
                 for f in range(n.value)]
 
-    def render(self, positions, scales, rotations, opacities, sh_0, sh_rest, settings: list[RasterizerSettings],
-               to_chw: bool = True, blur_periphery: bool = False, aaa_mode: bool = False, fast_math: bool = True,
-               images: list[torch.Tensor] | None = None, sync: bool = True) -> list[torch.Tensor]:
-        """Renders len(settings) views; K, SH bases, planes, scale and background of settings[0] apply."""
+    def _frame(self, positions, scales, rotations, opacities, sh_0, sh_rest, settings, to_chw, blur_periphery,
+               aaa_mode, fast_math, images):
+        """C structures of one frame: (keep-alive, primitives, views array, settings, images)."""
         dev = self.device
         keep = _Keep(dev)
         n, total_sh = _check_gaussians(positions, scales, rotations, opacities, sh_0, sh_rest)
@@ -355,6 +354,15 @@ class Renderer:
                                  keep.u32(s.fovea_mask_area_table, "fovea_mask_area_table"), int(s.width),
                                  int(s.height), float(s.focal_x), float(s.focal_y), float(s.center_x),
                                  float(s.center_y), images[i].data_ptr())
+        return keep, prims, views, st, images, n
+
+    def render(self, positions, scales, rotations, opacities, sh_0, sh_rest, settings: list[RasterizerSettings],
+               to_chw: bool = True, blur_periphery: bool = False, aaa_mode: bool = False, fast_math: bool = True,
+               images: list[torch.Tensor] | None = None, sync: bool = True) -> list[torch.Tensor]:
+        """Renders len(settings) views; K, SH bases, planes, scale and background of settings[0] apply."""
+        dev = self.device
+        keep, prims, views, st, images, n = self._frame(positions, scales, rotations, opacities, sh_0, sh_rest,
+                                                        settings, to_chw, blur_periphery, aaa_mode, fast_math, images)
         fn = self._libh.fhtgs_render_views_sync if sync else self._libh.fhtgs_render_views
         with torch.cuda.device(dev):
             _lib.check(fn(self.ctx, C.byref(prims), views, len(settings), C.byref(st), _stream_handle(dev)))
@@ -364,6 +372,64 @@ class Renderer:
         self._last_n = n
         self._last_sizes = [(int(s.width), int(s.height)) for s in settings]
         return images
+
+    # ---- batched frames: tuning, autotuner, captured frame graphs ----
+
+    def get_tuning(self) -> dict:
+        t = _lib.Tuning()
+        _lib.check(self._libh.fhtgs_context_get_tuning(self.ctx, C.byref(t)))
+        return dict(blend_warp_width=int(t.blend_warp_width), blend_blocks_per_sm=int(t.blend_blocks_per_sm),
+                    sort_items=int(t.sort_items))
+
+    def set_tuning(self, blend_warp_width: int = 8, blend_blocks_per_sm: int = 0, sort_items: int = 16):
+        """Kernel shapes of this context (identical images for every choice)."""
+        t = _lib.Tuning(int(blend_warp_width), int(blend_blocks_per_sm), int(sort_items))
+        _lib.check(self._libh.fhtgs_context_set_tuning(self.ctx, C.byref(t)))
+
+    def autotune(self, positions, scales, rotations, opacities, sh_0, sh_rest, settings: list[RasterizerSettings],
+                 to_chw: bool = True, blur_periphery: bool = False, aaa_mode: bool = False, fast_math: bool = True,
+                 repeats: int = 5) -> dict:
+        """Times the tuning candidates on this frame and keeps the fastest (see fhtgs_autotune)."""
+        keep, prims, views, st, images, n = self._frame(positions, scales, rotations, opacities, sh_0, sh_rest,
+                                                        settings, to_chw, blur_periphery, aaa_mode, fast_math, None)
+        best = _lib.Tuning()
+        ms = C.c_float(0.0)
+        with torch.cuda.device(self.device):
+            _lib.check(self._libh.fhtgs_autotune(self.ctx, C.byref(prims), views, len(settings), C.byref(st),
+                                                 int(repeats), C.byref(best), C.byref(ms),
+                                                 _stream_handle(self.device)))
+        self._last_views, self._last_n = len(settings), n
+        self._last_sizes = [(int(s.width), int(s.height)) for s in settings]
+        return dict(blend_warp_width=int(best.blend_warp_width), blend_blocks_per_sm=int(best.blend_blocks_per_sm),
+                    sort_items=int(best.sort_items), frame_ms=float(ms.value))
+
+    def capture(self, positions, scales, rotations, opacities, sh_0, sh_rest, settings: list[RasterizerSettings],
+                to_chw: bool = True, blur_periphery: bool = False, aaa_mode: bool = False, fast_math: bool = True,
+                images: list[torch.Tensor] | None = None, gaze: torch.Tensor | None = None,
+                capacity_headroom: float = 1.25) -> "FrameGraph":
+        """Captures one frame of len(settings) views into a CUDA graph (see fhtgs_frame_graph_create).
+
+        All tensors are used in place by every launch: update camera matrices, masks and
+        Gaussians with copy_() between launches.  `gaze`: optional float32 [n_views, 2] CUDA
+        tensor read at every launch (else the settings' host gaze is baked in).
+        """
+        keep, prims, views, st, images, n = self._frame(positions, scales, rotations, opacities, sh_0, sh_rest,
+                                                        settings, to_chw, blur_periphery, aaa_mode, fast_math, images)
+        gptr = None
+        if gaze is not None:
+            if gaze.device != self.device or gaze.dtype != torch.float32 or gaze.numel() != 2 * len(settings):
+                raise ValueError("gaze must be a float32 [n_views, 2] tensor on the renderer's device")
+            gaze = gaze.contiguous()
+            gptr = gaze.data_ptr()
+            keep.refs.append(gaze)
+        out = _lib.vp()
+        with torch.cuda.device(self.device):
+            _lib.check(self._libh.fhtgs_frame_graph_create(self.ctx, C.byref(prims), views, len(settings),
+                                                           C.byref(st), gptr, float(capacity_headroom),
+                                                           C.byref(out), _stream_handle(self.device)))
+        self._last_views, self._last_n = len(settings), n
+        self._last_sizes = [(int(s.width), int(s.height)) for s in settings]
+        return FrameGraph(self, out.value, keep, images)
 
     def frame_info(self, view: int = 0) -> dict:
         fi = _lib.FrameInfo()
@@ -404,3 +470,32 @@ class Renderer:
         out["values"] = out["values"][:m]
         out.update(info)
         return out
+
+
+class FrameGraph:
+    """A captured frame (fhtgs_frame_graph): `launch()` replays it on the current stream."""
+
+    def __init__(self, renderer: Renderer, handle: int, keep, images: list[torch.Tensor]):
+        self.renderer = renderer
+        self.handle = handle
+        self._keep = keep  # every tensor the graph reads or writes stays alive with it
+        self.images = images
+
+    def launch(self, sync: bool = False) -> list[torch.Tensor]:
+        r = self.renderer
+        with torch.cuda.device(r.device):
+            _lib.check(r._libh.fhtgs_frame_graph_launch(self.handle, _stream_handle(r.device)))
+            if sync:
+                torch.cuda.current_stream(r.device).synchronize()
+        return self.images
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.renderer._libh.fhtgs_frame_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

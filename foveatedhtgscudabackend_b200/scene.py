@@ -206,6 +206,32 @@ def make_stereo_views(width: int, height: int, ipd: float = 0.063, gaze_sigma: f
     return left, right
 
 
+BATCH_RESOLUTIONS = ((640, 480), (1280, 720), (1920, 1080), (2064, 2208))
+
+
+def make_batched_views(n_views: int = 64, seed: int = 0, radius=(4.0, 8.0), resolutions=BATCH_RESOLUTIONS,
+                       gaze_range: float = 0.8) -> list[View]:
+    """Cameras on a sphere around the origin looking at it, for batched rendering.
+
+    Directions uniform on the sphere (away from the poles, where the fixed up vector
+    degenerates), distance uniform in `radius`, resolution drawn uniformly from `resolutions`,
+    gaze uniform in [-gaze_range, gaze_range]^2 NDC per view.
+    """
+    rng = np.random.default_rng(seed + 104729)
+    views = []
+    for _ in range(n_views):
+        while True:
+            d = rng.normal(size=3)
+            d /= np.linalg.norm(d)
+            if abs(d[1]) < 0.95:
+                break
+        r = rng.uniform(*radius)
+        w, h = resolutions[int(rng.integers(len(resolutions)))]
+        g = rng.uniform(-gaze_range, gaze_range, size=2)
+        views.append(make_view(w, h, position=tuple(r * d), gaze_ndc=tuple(g)))
+    return views
+
+
 def random_visibility(grid_w: int, grid_h: int, p_visible: float, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
     return rng.random((grid_h, grid_w)) < p_visible

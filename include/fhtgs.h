@@ -231,6 +231,47 @@ fhtgs_status fhtgs_sort_instances_noalloc(const void* keys_in, const uint32_t* v
                                           void* keys_out, uint32_t* values_out, int64_t n,
                                           int32_t key_bytes, int32_t end_bit, void* stream);
 
+/* ---- batched frames: tuning, autotuner, captured frame graphs ----
+ * No counterpart in the reference (one view per blocking call, inference.cu:49-472).
+ *
+ * Tuning knobs of a context; every choice renders identical images (they change which pairs
+ * the blend culls as hopeless and how the sort is tiled, never a pixel's arithmetic):
+ *   blend_warp_width     pixels per warp row in the blend: 8 (8x4 pixels), 16 (16x2) or 4 (4x8)
+ *   blend_blocks_per_sm  persistent blend blocks per SM; 0 = as many as fit
+ *   sort_items           keys per thread of a radix-sort tile: 8, 12 or 16 (tile = 256 x items) */
+typedef struct fhtgs_tuning {
+    int32_t blend_warp_width;
+    int32_t blend_blocks_per_sm;
+    int32_t sort_items;
+} fhtgs_tuning;
+fhtgs_status fhtgs_context_set_tuning(fhtgs_context ctx, const fhtgs_tuning* tuning);
+fhtgs_status fhtgs_context_get_tuning(fhtgs_context ctx, fhtgs_tuning* tuning);
+/* Autotuner: renders the given frame with each candidate and keeps the fastest.  The blend knobs
+ * are chosen first by the blend's CUDA-event time (width x blocks), then sort_items by the
+ * sort's; each candidate is timed as the median of `repeats` (1..32) frames after one warm-up
+ * frame.  The winner becomes the context's tuning and is returned with its median frame time.
+ * Blocks the calling thread; profiling is switched on for the search and restored after. */
+fhtgs_status fhtgs_autotune(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views,
+                            int32_t n_views, const fhtgs_settings* settings, int32_t repeats,
+                            fhtgs_tuning* best, float* best_frame_ms, void* stream);
+
+/* A frame of n views captured once into a CUDA graph and replayed by one launch.  Everything the
+ * views point to is baked in by address: the caller updates camera matrices, masks and
+ * Gaussians in place between launches and reads the images from the same buffers.  Gaze:
+ * `gaze_device` = NULL keeps the host values of views[]; otherwise [n_views][2] floats in device
+ * memory are read (clamped and rounded as on the host) at every launch.  Creation renders the
+ * frame eagerly first and sizes the instance capacity at `capacity_headroom` (>= 1) times the
+ * largest per-view count, so that moving cameras fit; a launch whose instances exceed it sets
+ * `overflow` in fhtgs_get_frame_info (create the graph again then).  A graph belongs to its
+ * context: launching it after the context's arena moved (a larger eager frame, a reserve, a
+ * tuning change that grows it) fails with FHTGS_ERR_NOT_READY.  One frame at a time per context. */
+typedef struct fhtgs_frame_graph_s* fhtgs_frame_graph;
+fhtgs_status fhtgs_frame_graph_create(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views,
+                                      int32_t n_views, const fhtgs_settings* settings, const float* gaze_device,
+                                      float capacity_headroom, fhtgs_frame_graph* out, void* stream);
+fhtgs_status fhtgs_frame_graph_launch(fhtgs_frame_graph graph, void* stream);
+fhtgs_status fhtgs_frame_graph_destroy(fhtgs_frame_graph graph);
+
 /* ---- tile masks on the device ----
  * No counterpart in the reference, which takes the three mask tensors precomputed by the
  * calling framework (torch_bindings/rasterization.py:22-43; read at
