@@ -58,8 +58,9 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--cpu-budget-s", type=float, default=30.0, help="upper bound of the CPU baseline sample")
-    ap.add_argument("--workload", choices=["stereo", "batched"], default="stereo",
-                    help="stereo: the headline stereo frame; batched: 64 mixed-resolution cameras of a 3M scene")
+    ap.add_argument("--workload", choices=["stereo", "batched", "precision"], default="stereo",
+                    help="stereo: the headline stereo frame; batched: 64 mixed-resolution cameras of a 3M scene; "
+                         "precision: 6M-Gaussian stereo frame with fp16/bf16 attribute storage")
     ap.add_argument("--n-views", type=int, default=64, help="cameras per batch (batched workload)")
     return ap.parse_args(argv)
 
@@ -400,6 +401,87 @@ def run_batched(a, world, rank, local):
 
 
 # ------------------------------------------------------------------------------------------
+# reduced-precision storage workload
+# ------------------------------------------------------------------------------------------
+def run_precision(a, world, rank, local):
+    """6M Gaussians SH3, stereo 2 x 2064x2208, K = 8: the scene stored as fp32 and as the
+    reduced-precision format (positions fp32; scales, quaternions, opacities fp16; SH bf16;
+    fp32 arithmetic).  `value` = frames/s of the reduced-precision scene; beside it the fp32
+    scene's frames/s and the image error of the one against the other (PSNR, max-abs)."""
+    import torch
+
+    import foveatedhtgscudabackend_b200 as F
+    from foveatedhtgscudabackend_b200 import scene
+
+    dev = torch.device("cuda", local)
+    n_gauss = a.n_gaussians if a.n_gaussians != 1_000_000 else 6_000_000
+    g = scene.make_gaussians(n_gauss, a.sh_degree, seed=0)
+    left, right = scene.make_stereo_views(a.width, a.height, seed=rank)
+    active = (a.sh_degree + 1) ** 2
+    st = [F.settings_from_view(v, K=a.K, active_sh_bases=active, device=dev) for v in (left, right)]
+    full = F.gaussians_to_torch(g, dev)
+    half = F.to_half_storage(*full)
+    bytes_full = sum(t.numel() * t.element_size() for t in full)
+    bytes_half = sum(t.numel() * t.element_size() for t in half)
+    del g
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for name, gt in (("fp32", full), ("half", half)):
+        r = F.Renderer(dev)
+        imgs = [torch.empty((3, v.height, v.width), device=dev) for v in (left, right)]
+        r.render(*gt, st, images=imgs, sync=True)
+        for _ in range(max(a.warmup, 0)):
+            r.render(*gt, st, images=imgs, sync=False)
+        r.set_profiling(True)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
+        clocks = ClockSampler(local) if name == "half" else None
+        if clocks:
+            clocks.start()
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        ev[0].record(stream)
+        launches0 = r.launch_count()
+        for k in range(a.steps):
+            r.render(*gt, st, images=imgs, sync=False)
+            ev[k + 1].record(stream)
+        torch.cuda.synchronize(dev)
+        launches = r.launch_count() - launches0
+        clk = clocks.stop() if clocks else None
+        total = max_over_ranks(ev[0].elapsed_time(ev[a.steps]), world)
+        per = sorted(ev[k].elapsed_time(ev[k + 1]) for k in range(a.steps))
+        hist = r.stage_history(min(a.steps, 64))
+        overflow = any(r.frame_info(i)["overflow"] for i in range(2))
+        out[name] = dict(fps=world * a.steps / (total / 1000.0), p50=float(np.percentile(per, 50)),
+                         p99=float(np.percentile(per, 99)), images=[x.clone() for x in imgs],
+                         stages={k: round(statistics.mean(h[k] for h in hist), 4) for k in hist[0]},
+                         launches=launches, clk=clk, overflow=overflow)
+        r.close()
+    err = []
+    for x, y in zip(out["half"]["images"], out["fp32"]["images"]):
+        mse = float(((x.double() - y.double()) ** 2).mean())
+        err.append({"psnr_db": round(10 * np.log10(1.0 / mse), 2) if mse > 0 else float("inf"),
+                    "max_abs": round(float((x - y).abs().max()), 5)})
+    if rank != 0:
+        return None
+    h, f = out["half"], out["fp32"]
+    return {
+        "metric": "stereo frames/s with fp16/bf16 Gaussian storage (fp32 arithmetic)", "value": round(h["fps"], 3),
+        "unit": "frames/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": round(1000.0 / h["fps"] * world, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f16/bf16 storage, f32 compute", "data": "synthetic",
+        "config": {"workload": f"precision_stereo_{n_gauss // 1000}k_sh{a.sh_degree}_2x{a.width}x{a.height}_k{a.K}",
+                   "n_gaussians": n_gauss, "storage": "positions fp32; scales, rotations, opacities fp16; SH bf16",
+                   "scene_bytes": {"fp32": bytes_full, "half": bytes_half},
+                   "foveation": "reference constants", "l2": "inputs larger than L2"},
+        "latency_ms": {"p50": round(h["p50"], 4), "p99": round(h["p99"], 4)},
+        "fp32_storage": {"frames_per_s": round(f["fps"], 3), "p50_ms": round(f["p50"], 4), "stage_ms": f["stages"]},
+        "stage_ms": h["stages"],
+        "error_vs_fp32_storage": err,
+        "gpu_launches": int(h["launches"]), "overflow": h["overflow"] or f["overflow"], "clocks": h["clk"],
+    }
+
+
+# ------------------------------------------------------------------------------------------
 # reference arm: the reference algorithm on the host cores
 # ------------------------------------------------------------------------------------------
 def run_reference(a, world, rank):
@@ -429,6 +511,8 @@ def main(argv=None) -> int:
             line = run_reference(a, world, rank)
         elif a.workload == "batched":
             line = run_batched(a, world, rank, local)
+        elif a.workload == "precision":
+            line = run_precision(a, world, rank, local)
         else:
             line = run_ours(a, world, rank, local)
         if line is not None:

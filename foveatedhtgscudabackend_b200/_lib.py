@@ -41,7 +41,11 @@ class FhtgsError(RuntimeError):
 
 class Primitives(C.Structure):
     _fields_ = [("positions", vp), ("scales", vp), ("rotations", vp), ("opacities", vp), ("sh_0", vp),
-                ("sh_rest", vp), ("n_primitives", c_i32), ("total_sh_bases", c_i32)]
+                ("sh_rest", vp), ("n_primitives", c_i32), ("total_sh_bases", c_i32), ("storage", c_i32)]
+
+
+STORAGE_FP32 = 0
+STORAGE_HALF = 1
 
 
 class View(C.Structure):

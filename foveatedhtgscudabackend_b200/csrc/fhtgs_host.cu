@@ -170,6 +170,8 @@ fhtgs_status validate(const fhtgs_primitives* p, const fhtgs_view* views, int n_
     if (n_views <= 0 || n_views > 255) return fail(FHTGS_ERR_INVALID_ARGUMENT, "n_views must be in [1, 255]");
     if (p->n_primitives < 0) return fail(FHTGS_ERR_INVALID_ARGUMENT, "n_primitives must be >= 0");
     if (p->total_sh_bases < 0) return fail(FHTGS_ERR_INVALID_ARGUMENT, "total_sh_bases must be >= 0");
+    if (p->storage != FHTGS_STORAGE_FP32 && p->storage != FHTGS_STORAGE_HALF)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "unknown storage format");
     if (p->n_primitives > 0 && (!p->positions || !p->scales || !p->rotations || !p->opacities || !p->sh_0))
         return fail(FHTGS_ERR_INVALID_ARGUMENT, "null Gaussian attribute pointer");
     if (s->active_sh_bases > 1 && s->active_sh_bases > p->total_sh_bases + 1)
@@ -320,7 +322,8 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
         p.image = v.image;
         p.work = s->blur_periphery ? reinterpret_cast<float*>(A + L.temp_offsets[i]) : v.image;
     }
-    Gaussians gs{prims->positions, prims->scales, prims->rotations, prims->opacities, prims->sh_0, prims->sh_rest};
+    Gaussians gs{prims->positions, prims->scales, prims->rotations, prims->opacities, prims->sh_0, prims->sh_rest,
+                 prims->storage == FHTGS_STORAGE_HALF ? 1 : 0};
     const KernelSet& ks = s->fast_math ? kernels_fast() : kernels_ieee();
 
     const bool prof = ctx->profile && !ctx->capturing;
@@ -811,7 +814,8 @@ static fhtgs_status mono_common(fhtgs_context ctx, int fast, const float* positi
                                 int32_t to_chw, int32_t blur_periphery, int32_t anti_aliasing, float* image,
                                 void* stream) {
     if (!ctx) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null context");
-    fhtgs_primitives p{positions, scales, rotations, opacities, sh_0, sh_rest, n_primitives, total_sh_bases};
+    fhtgs_primitives p{positions, scales, rotations, opacities, sh_0, sh_rest, n_primitives, total_sh_bases,
+                       FHTGS_STORAGE_FP32};
     fhtgs_view v{};
     v.M = M; v.VPM = VPM; v.VPR_inv = VPR_inv; v.cam_position = cam_position;
     v.gaze_x = gaze_x; v.gaze_y = gaze_y;
@@ -876,7 +880,8 @@ fhtgs_status fhtgs_render_stereo(
     float focal_y_right, float center_x_right, float center_y_right, int32_t to_chw, int32_t blur_periphery,
     int32_t anti_aliasing, float* image_left, float* image_right, void* stream) {
     if (!ctx) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null context");
-    fhtgs_primitives p{positions, scales, rotations, opacities, sh_0, sh_rest, n_primitives, total_sh_bases};
+    fhtgs_primitives p{positions, scales, rotations, opacities, sh_0, sh_rest, n_primitives, total_sh_bases,
+                       FHTGS_STORAGE_FP32};
     fhtgs_view v[2] = {};
     v[0].M = M_left; v[0].VPM = VPM_left; v[0].VPR_inv = VPR_inv_left; v[0].cam_position = cam_position_left;
     v[0].gaze_x = gaze_x_left; v[0].gaze_y = gaze_y_left;

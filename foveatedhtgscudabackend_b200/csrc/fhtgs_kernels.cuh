@@ -17,6 +17,9 @@
 //              tiles (periphery), persistent blocks pulling tiles from a work counter
 //   compose    periphery bilinear upsampling / blur and blended-ring cross-fade
 #pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "fhtgs_math.cuh"
 #include "fhtgs_types.cuh"
 
@@ -246,8 +249,19 @@ constexpr float kC3a = 0.59004358992664352f, kC3b = 1.7701307697799304f, kC3c = 
                 kC3d = 0.45704579946446572f, kC3e = 2.2852289973223288f, kC3f = 1.865881662950577f,
                 kC3g = 1.1195289977703462f, kC3h = 1.4453057213202769f;
 
-__device__ __forceinline__ float3 sh_to_rgb(const float* __restrict__ sh0, const float* __restrict__ rest,
+// Attribute loads of the two storage formats, widened to float32 (exact conversions).
+__device__ __forceinline__ float ldf(const float* p) { return *p; }
+__device__ __forceinline__ float ldf(const __half* p) { return __half2float(*p); }
+__device__ __forceinline__ float ldf(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+template <typename T>
+__device__ __forceinline__ float3 ld3t(const T* p) { return make_float3(ldf(p), ldf(p + 1), ldf(p + 2)); }
+template <typename T>
+__device__ __forceinline__ float4 ld4t(const T* p) { return make_float4(ldf(p), ldf(p + 1), ldf(p + 2), ldf(p + 3)); }
+
+template <typename ShT>
+__device__ __forceinline__ float3 sh_to_rgb(const ShT* __restrict__ sh0, const ShT* __restrict__ rest,
                                             float3 pos, float3 cam, int active) {
+    auto ld3 = [](const ShT* p) { return ld3t(p); };
     float3 res = 0.5f + kC0 * ld3(sh0);
     if (active > 1) {
         const float3 d = normalize(pos - cam);
@@ -478,19 +492,26 @@ __device__ __forceinline__ bool transform_and_cull_aaa(const ViewParams& vp, con
     return n == 0;
 }
 
+// AttrT: element type of scales/rotations/opacities; ShT: of sh_0/sh_rest.
+template <typename AttrT, typename ShT>
 __global__ void __launch_bounds__(kPrimBlock) preprocess_kernel(FrameParams fp, FrameBuffers fb, Gaussians g) {
     __shared__ uint32_t s_warp[33];
     const int i = blockIdx.x * kPrimBlock + threadIdx.x;
     const bool valid = i < fp.n_prims;
     const int ii = valid ? i : 0;
+    const AttrT* scales = reinterpret_cast<const AttrT*>(g.scales);
+    const AttrT* rotations = reinterpret_cast<const AttrT*>(g.rotations);
+    const AttrT* opacities = reinterpret_cast<const AttrT*>(g.opacities);
+    const ShT* sh_0 = reinterpret_cast<const ShT*>(g.sh_0);
+    const ShT* sh_rest = reinterpret_cast<const ShT*>(g.sh_rest);
     float3 pos = make_float3(0.f, 0.f, 0.f), scale = pos;
     float4 quat = make_float4(1.f, 0.f, 0.f, 0.f);
     float op = 0.0f;
     if (valid) {
         pos = ld3(g.positions + 3 * static_cast<size_t>(ii));
-        scale = ld3(g.scales + 3 * static_cast<size_t>(ii));
-        quat = ld4(g.rotations + 4 * static_cast<size_t>(ii));
-        op = g.opacities[ii];
+        scale = ld3t(scales + 3 * static_cast<size_t>(ii));
+        quat = ld4t(rotations + 4 * static_cast<size_t>(ii));
+        op = ldf(opacities + ii);
     }
     const size_t N = static_cast<size_t>(fp.n_prims);
     for (int v = 0; v < fp.n_views; ++v) {
@@ -509,8 +530,8 @@ __global__ void __launch_bounds__(kPrimBlock) preprocess_kernel(FrameParams fp, 
             if (!culled) {
                 fb.bounds[o] = make_ushort4(static_cast<unsigned short>(b.x), static_cast<unsigned short>(b.y),
                                             static_cast<unsigned short>(b.z), static_cast<unsigned short>(b.w));
-                const float3 rgb = sh_to_rgb(g.sh_0 + 3 * static_cast<size_t>(ii),
-                                             g.sh_rest + static_cast<size_t>(3) * fp.total_sh * ii, pos, xyz(vp.cam),
+                const float3 rgb = sh_to_rgb(sh_0 + 3 * static_cast<size_t>(ii),
+                                             sh_rest + static_cast<size_t>(3) * fp.total_sh * ii, pos, xyz(vp.cam),
                                              fp.active_sh);
                 float4* r = fb.rec + 4 * o;
                 r[0] = P1;
@@ -531,7 +552,8 @@ __global__ void __launch_bounds__(kPrimBlock) preprocess_kernel(FrameParams fp, 
 
 int launch_preprocess(const FrameParams& fp, const FrameBuffers& fb, const Gaussians& g, cudaStream_t s) {
     if (fp.n_blocks_prim == 0) return 0;
-    preprocess_kernel<<<fp.n_blocks_prim, kPrimBlock, 0, s>>>(fp, fb, g);
+    if (g.half) preprocess_kernel<__half, __nv_bfloat16><<<fp.n_blocks_prim, kPrimBlock, 0, s>>>(fp, fb, g);
+    else preprocess_kernel<float, float><<<fp.n_blocks_prim, kPrimBlock, 0, s>>>(fp, fb, g);
     return 1;
 }
 

@@ -94,6 +94,8 @@ struct FrameStatus {
     uint32_t pad;
 };
 
+// Attribute arrays; with `half` set, scales/rotations/opacities hold fp16 and sh_0/sh_rest
+// bfloat16 values behind these pointers (positions stay float32).
 struct Gaussians {
     const float* positions;
     const float* scales;
@@ -101,6 +103,7 @@ struct Gaussians {
     const float* opacities;
     const float* sh_0;
     const float* sh_rest;
+    int half;
 };
 
 // All per-frame device buffers (arena carve-up); arrays are [view][...] with the strides

@@ -89,6 +89,17 @@ class _Keep:
         self.refs.append(t)
         return t.data_ptr() if t.numel() else 0
 
+    def typed(self, t: torch.Tensor, name: str, dtype: torch.dtype) -> int:
+        if not isinstance(t, torch.Tensor):
+            raise TypeError(f"{name} must be a torch.Tensor")
+        if t.device != self.device:
+            raise ValueError(f"{name} must be on {self.device}, got {t.device}")
+        if t.dtype != dtype:
+            raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+        t = t.contiguous()
+        self.refs.append(t)
+        return t.data_ptr() if t.numel() else 0
+
     def u32(self, t: torch.Tensor, name: str) -> int:
         if not isinstance(t, torch.Tensor):
             raise TypeError(f"{name} must be a torch.Tensor")
@@ -332,9 +343,18 @@ class Renderer:
         dev = self.device
         keep = _Keep(dev)
         n, total_sh = _check_gaussians(positions, scales, rotations, opacities, sh_0, sh_rest)
-        prims = _lib.Primitives(keep.f32(positions, "positions"), keep.f32(scales, "scales"),
-                                keep.f32(rotations, "rotations"), keep.f32(opacities, "opacities"),
-                                keep.f32(sh_0, "sh_0"), keep.f32(sh_rest, "sh_rest"), n, total_sh)
+        if isinstance(scales, torch.Tensor) and scales.dtype == torch.float16:
+            # reduced-precision storage: fp16 scales/rotations/opacities, bf16 SH, fp32 positions
+            h, b = torch.float16, torch.bfloat16
+            prims = _lib.Primitives(keep.f32(positions, "positions"), keep.typed(scales, "scales", h),
+                                    keep.typed(rotations, "rotations", h), keep.typed(opacities, "opacities", h),
+                                    keep.typed(sh_0, "sh_0", b), keep.typed(sh_rest, "sh_rest", b), n, total_sh,
+                                    _lib.STORAGE_HALF)
+        else:
+            prims = _lib.Primitives(keep.f32(positions, "positions"), keep.f32(scales, "scales"),
+                                    keep.f32(rotations, "rotations"), keep.f32(opacities, "opacities"),
+                                    keep.f32(sh_0, "sh_0"), keep.f32(sh_rest, "sh_rest"), n, total_sh,
+                                    _lib.STORAGE_FP32)
         s0 = settings[0]
         bg_type = s0.background_model.value
         tw, th = _texture_size(bg_type, s0.background_model_data)

@@ -8,11 +8,31 @@ from . import scene as _scene
 from .rasterization import BackgroundModel, RasterizerSettings
 
 
-def gaussians_to_torch(g: _scene.Gaussians, device="cuda") -> tuple[torch.Tensor, ...]:
-    """(positions, scales, rotations, opacities, sh_0, sh_rest) as float32 tensors on `device`."""
+def gaussians_to_torch(g: _scene.Gaussians, device="cuda", storage: str = "fp32") -> tuple[torch.Tensor, ...]:
+    """(positions, scales, rotations, opacities, sh_0, sh_rest) on `device`.
+
+    storage "fp32": every attribute float32.  "half": positions float32; scales, rotations and
+    opacities float16; sh_0 and sh_rest bfloat16 (rounded to nearest even from float32).
+    """
     def t(a):
         return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(device)
-    return (t(g.positions), t(g.scales), t(g.rotations), t(g.opacities), t(g.sh_0), t(g.sh_rest))
+    out = (t(g.positions), t(g.scales), t(g.rotations), t(g.opacities), t(g.sh_0), t(g.sh_rest))
+    if storage == "fp32":
+        return out
+    if storage != "half":
+        raise ValueError(f"unknown storage {storage!r}")
+    return to_half_storage(*out)
+
+
+def to_half_storage(positions, scales, rotations, opacities, sh_0, sh_rest) -> tuple[torch.Tensor, ...]:
+    """The reduced-precision storage of float32 Gaussians (see gaussians_to_torch)."""
+    return (positions.float().contiguous(), scales.half().contiguous(), rotations.half().contiguous(),
+            opacities.half().contiguous(), sh_0.bfloat16().contiguous(), sh_rest.bfloat16().contiguous())
+
+
+def from_half_storage(positions, scales, rotations, opacities, sh_0, sh_rest) -> tuple[torch.Tensor, ...]:
+    """Float32 copies of reduced-precision Gaussians (exact widening)."""
+    return tuple(x.float().contiguous() for x in (positions, scales, rotations, opacities, sh_0, sh_rest))
 
 
 def settings_from_view(v: _scene.View, *, K: int = 8, active_sh_bases: int = 16, scale_modifier: float = 1.0,

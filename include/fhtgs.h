@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FHTGS_ABI_VERSION 1
+#define FHTGS_ABI_VERSION 2
 
 typedef enum {
     FHTGS_OK = 0,
@@ -50,7 +50,18 @@ typedef enum {
 
 typedef struct fhtgs_context_s* fhtgs_context;
 
-/* Gaussians (device, float32, contiguous, activated parameters). */
+/* Storage formats of the Gaussian attributes (fhtgs_primitives.storage).  Either way every
+ * attribute is widened to float32 when read and all arithmetic is float32. */
+typedef enum {
+    FHTGS_STORAGE_FP32 = 0,  /* all attributes float32 (the reference's format)            */
+    FHTGS_STORAGE_HALF = 1   /* positions float32; scales, rotations, opacities IEEE fp16;
+                                sh_0 and sh_rest bfloat16 (124 instead of 236 B per SH3
+                                Gaussian)                                                  */
+} fhtgs_storage;
+
+/* Gaussians (device, contiguous, activated parameters; element type per `storage`).  The
+ * pointers are typed float for the FP32 format; for FHTGS_STORAGE_HALF pass the 16-bit arrays
+ * cast to these pointer types. */
 typedef struct {
     const float* positions;  /* [N,3]                                   */
     const float* scales;     /* [N,3] linear                            */
@@ -60,6 +71,7 @@ typedef struct {
     const float* sh_rest;    /* [N,S,3], may be NULL when S == 0        */
     int32_t n_primitives;    /* N                                       */
     int32_t total_sh_bases;  /* S = sh_rest.size(1)                     */
+    int32_t storage;         /* fhtgs_storage; 0 = FP32                 */
 } fhtgs_primitives;
 
 /* One camera and its output image. */
