@@ -58,10 +58,16 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--cpu-budget-s", type=float, default=30.0, help="upper bound of the CPU baseline sample")
-    ap.add_argument("--workload", choices=["stereo", "batched", "precision"], default="stereo",
+    ap.add_argument("--workload", choices=["stereo", "batched", "precision", "served"], default="stereo",
                     help="stereo: the headline stereo frame; batched: 64 mixed-resolution cameras of a 3M scene; "
-                         "precision: 6M-Gaussian stereo frame with fp16/bf16 attribute storage")
+                         "precision: 6M-Gaussian stereo frame with fp16/bf16 attribute storage; served: a Poisson "
+                         "stream of stereo requests against 3 resident scenes through the request server")
     ap.add_argument("--n-views", type=int, default=64, help="cameras per batch (batched workload)")
+    ap.add_argument("--duration", type=float, default=10.0, help="seconds of arrivals (served workload)")
+    ap.add_argument("--rate", type=float, default=240.0, help="request arrivals per second (served workload)")
+    ap.add_argument("--slots", type=int, default=2, help="frames in flight (served workload)")
+    ap.add_argument("--max-batch", type=int, default=8, help="requests per frame (served workload)")
+    ap.add_argument("--no-plain", action="store_true", help="served workload: skip the plain per-request path")
     return ap.parse_args(argv)
 
 
@@ -482,6 +488,157 @@ def run_precision(a, world, rank, local):
 
 
 # ------------------------------------------------------------------------------------------
+# served stream: resident scenes, Poisson arrivals, continuous batching vs one call per request
+# ------------------------------------------------------------------------------------------
+SERVED_SCENES = (500_000, 2_000_000, 4_000_000)
+
+
+def run_served(a, world, rank, local):
+    """3 resident scenes (0.5M, 2M, 4M Gaussians, SH3, seeds 1-3); stereo requests arriving
+    Poisson at `--rate` per second for `--duration` s, each with a uniformly drawn scene, one
+    resolution per request from {1440x1584, 2064x2208} per eye, a random head pose (sphere,
+    r in [4, 8]) and gaze; K = 8, fast-math, 150 GB budget.  The same trace runs through
+    (a) the request server (continuous batching over `--slots` frames in flight) — `value`,
+    and (b) the plain per-request path: one blocking drop-in `_C_stereo.render` call per
+    request, in arrival order.  Latency = GPU completion - scheduled arrival.  Both paths
+    also drain the whole trace submitted at once (saturated requests/s)."""
+    import torch
+
+    import foveatedhtgscudabackend_b200 as F
+    from foveatedhtgscudabackend_b200 import _C_stereo, scene
+    from foveatedhtgscudabackend_b200.serving import Server
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    scenes = [F.gaussians_to_torch(scene.make_gaussians(n, a.sh_degree, seed=i + 1), dev)
+              for i, n in enumerate(SERVED_SCENES)]
+    active = (a.sh_degree + 1) ** 2
+    trace = scene.make_served_requests(a.duration, a.rate, len(scenes), seed=rank)
+    warm = scene.make_served_requests(1.0, 96.0, len(scenes), seed=1000 + rank)
+    n_req = len(trace)
+
+    srv = Server(dev, hbm_budget_bytes=150e9, max_in_flight=a.slots, max_batch_requests=a.max_batch)
+    ids = [srv.add_scene(*gt, K=a.K, active_sh_bases=active) for gt in scenes]
+
+    def drain_all(expect):
+        got = 0
+        while got < expect:
+            cs = srv.poll(max_completions=256, wait_ms=1000)
+            if not cs:
+                raise RuntimeError("server made no progress")
+            for c in cs:
+                if not c.ok:
+                    raise RuntimeError(f"request failed: {c.message}")
+                srv.release(c.ticket)
+                got += 1
+        return got
+
+    # warm-up (untimed): full-size frames of every scene size the slot arenas and output pool
+    for rep in range(2):
+        srv.pause()
+        for t, si, l, r in warm:
+            srv.submit(ids[si], [l, r])
+        srv.resume()
+        drain_all(len(warm))
+
+    prepared = [srv.prepare(ids[si], [l, r], tag=k) for k, (t, si, l, r) in enumerate(trace)]
+    stats0 = srv.stats()
+    clocks = ClockSampler(local)
+    clocks.start()
+    # (a) server, Poisson replay
+    t0 = srv.clock_ms() + 20.0
+    arrive = [t0 + 1000.0 * t for t, *_ in trace]
+    lat_s = [0.0] * n_req
+    frame_views = []
+    i = done = 0
+    last_done = t0
+    while done < n_req:
+        now = srv.clock_ms()
+        while i < n_req and arrive[i] <= now:
+            srv.submit_prepared(prepared[i])
+            i += 1
+        wait = int(min(max(arrive[i] - srv.clock_ms() - 1.0, 0.0), 5.0)) if i < n_req else 5
+        for c in srv.poll(max_completions=256, wait_ms=wait):
+            if not c.ok:
+                raise RuntimeError(f"request failed: {c.message}")
+            lat_s[c.tag] = c.done_ms - arrive[c.tag]
+            last_done = max(last_done, c.done_ms)
+            frame_views.append(c.frame_views)
+            srv.release(c.ticket)
+            done += 1
+    served_s = (last_done - t0) / 1000.0
+    stats1 = srv.stats()
+    # saturated: the whole trace at once
+    srv.pause()
+    ts = srv.clock_ms()
+    for p in prepared:
+        srv.submit_prepared(p)
+    srv.resume()
+    got = 0
+    sat_done = ts
+    while got < n_req:
+        for c in srv.poll(max_completions=256, wait_ms=1000):
+            sat_done = max(sat_done, c.done_ms)
+            srv.release(c.ticket)
+            got += 1
+    served_sat = n_req / ((sat_done - ts) / 1000.0)
+    clk = clocks.stop()
+    srv.close()
+
+    # (b) plain per-request path on the same trace (device settings prepared beforehand)
+    pct = lambda x, q: round(float(np.percentile(x, q)), 3)
+    plain = None
+    if not a.no_plain:
+        sts = [[F.settings_from_view(v, K=a.K, active_sh_bases=active, device=dev) for v in (l, r)]
+               for t, si, l, r in trace]
+        for t, si, l, r in warm[:6]:
+            w = [F.settings_from_view(v, K=a.K, active_sh_bases=active, device=dev) for v in (l, r)]
+            _C_stereo.render(*scenes[si], *w[0].as_tuple(), *w[1].as_tuple(), True, False, False)
+        torch.cuda.synchronize(dev)
+        clock = time.perf_counter
+        t0p = 1000.0 * clock() + 20.0
+        lat_p = []
+        for k, (t, si, l, r) in enumerate(trace):
+            arr = t0p + 1000.0 * t
+            while 1000.0 * clock() < arr:
+                pass
+            _C_stereo.render(*scenes[si], *sts[k][0].as_tuple(), *sts[k][1].as_tuple(), True, False, False)
+            lat_p.append(1000.0 * clock() - arr)
+        plain_s = (1000.0 * clock() - t0p) / 1000.0
+        ts = clock()
+        for k, (t, si, l, r) in enumerate(trace):
+            _C_stereo.render(*scenes[si], *sts[k][0].as_tuple(), *sts[k][1].as_tuple(), True, False, False)
+        plain_sat = n_req / (clock() - ts)
+        plain = {"api": "foveatedhtgscudabackend_b200._C_stereo.render, one blocking call per request",
+                 "requests_per_s": round(n_req / plain_s, 2), "p50_ms": pct(lat_p, 50), "p99_ms": pct(lat_p, 99),
+                 "max_ms": round(max(lat_p), 3), "saturated_requests_per_s": round(plain_sat, 2)}
+
+    if rank != 0:
+        return None
+    return {
+        "metric": "served stereo requests/s & p50/p99 latency vs plain per-request path (Poisson arrivals)",
+        "value": round(n_req / served_s, 2), "unit": "requests/s", "n_gpus": world, "steps": n_req, "warmup": 2 * len(warm),
+        "ms_per_step": round(1000.0 * served_s / n_req, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"served_{'_'.join(str(n // 1000) + 'k' for n in SERVED_SCENES)}_sh{a.sh_degree}_poisson{a.rate:g}",
+                   "scenes": list(SERVED_SCENES), "rate_per_s": a.rate, "duration_s": a.duration, "requests": n_req,
+                   "resolutions_per_eye": "uniform from 1440x1584, 2064x2208", "K": a.K,
+                   "head_pose": "sphere r in [4, 8] looking at the origin; gaze N(0, 0.1) NDC",
+                   "hbm_budget_gb": 150, "slots": a.slots, "max_batch_requests": a.max_batch,
+                   "l2": "inputs larger than L2"},
+        "latency_ms": {"p50": pct(lat_s, 50), "p99": pct(lat_s, 99), "max": round(max(lat_s), 3)},
+        "plain_path": plain,
+        "saturated_requests_per_s": round(served_sat, 2),
+        "throughput_vs_plain": round((n_req / served_s) / plain["requests_per_s"], 3) if plain else None,
+        "saturated_vs_plain": round(served_sat / plain["saturated_requests_per_s"], 3) if plain else None,
+        "mean_frame_views": round(float(np.mean(frame_views)), 2),
+        "server": {k: stats1[k] - stats0.get(k, 0) if k in ("frames", "views", "retries", "admission_waits") else stats1[k]
+                   for k in ("frames", "views", "retries", "admission_waits", "peak_resident_bytes", "max_frame_requests")},
+        "clocks": clk,
+    }
+
+
+# ------------------------------------------------------------------------------------------
 # reference arm: the reference algorithm on the host cores
 # ------------------------------------------------------------------------------------------
 def run_reference(a, world, rank):
@@ -513,6 +670,8 @@ def main(argv=None) -> int:
             line = run_batched(a, world, rank, local)
         elif a.workload == "precision":
             line = run_precision(a, world, rank, local)
+        elif a.workload == "served":
+            line = run_served(a, world, rank, local)
         else:
             line = run_ours(a, world, rank, local)
         if line is not None:

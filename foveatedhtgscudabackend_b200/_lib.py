@@ -78,6 +78,34 @@ class Tuning(C.Structure):
     _fields_ = [("blend_warp_width", c_i32), ("blend_blocks_per_sm", c_i32), ("sort_items", c_i32)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", c_i32), ("max_in_flight", c_i32), ("max_batch_requests", c_i32), ("reserved", c_i32),
+                ("hbm_budget_bytes", C.c_int64)]
+
+
+class Eye(C.Structure):
+    _fields_ = [("M", c_f * 12), ("VPM", c_f * 16), ("VPR_inv", c_f * 16), ("cam_position", c_f * 3),
+                ("gaze_x", c_f), ("gaze_y", c_f), ("width", c_i32), ("height", c_i32), ("focal_x", c_f),
+                ("focal_y", c_f), ("center_x", c_f), ("center_y", c_f), ("visibility_mask", vp),
+                ("visibility_mask_area_table", vp), ("fovea_mask_area_table", vp), ("image", vp)]
+
+
+class Request(C.Structure):
+    _fields_ = [("scene", c_i32), ("n_eyes", c_i32), ("tag", C.c_uint64), ("ready_event", vp), ("eyes", Eye * 2)]
+
+
+class Completion(C.Structure):
+    _fields_ = [("ticket", C.c_int64), ("tag", C.c_uint64), ("status", c_i32), ("frame_views", c_i32),
+                ("submit_ms", C.c_double), ("launch_ms", C.c_double), ("done_ms", C.c_double),
+                ("images", vp * 2), ("message", C.c_char * 96)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("submitted", "completed", "failed", "frames", "views", "retries", "queued",
+                                         "in_flight", "resident_bytes", "peak_resident_bytes", "admission_waits",
+                                         "max_frame_requests")]
+
+
 # Exported symbols and their signatures (mirrors include/fhtgs.h).
 _MONO_ARGS = [vp, vp, vp, vp, vp, vp, vp, c_i32, c_i32, vp, vp, vp, vp, c_f, c_f, vp, vp, vp, vp, c_i32, c_i32,
               c_i32, c_i32, c_i32, c_i32, c_i32, c_f, c_f, c_f, c_f, c_f, c_f, c_f, c_i32, c_i32, c_i32, vp, vp]
@@ -113,6 +141,17 @@ SIGNATURES = {
                                   C.POINTER(vp), vp], c_i32),
     "fhtgs_frame_graph_launch": ([vp, vp], c_i32),
     "fhtgs_frame_graph_destroy": ([vp], c_i32),
+    "fhtgs_server_create": ([C.POINTER(ServerConfig), C.POINTER(vp)], c_i32),
+    "fhtgs_server_destroy": ([vp], c_i32),
+    "fhtgs_server_add_scene": ([vp, C.POINTER(Primitives), C.POINTER(Settings), C.POINTER(c_i32)], c_i32),
+    "fhtgs_server_remove_scene": ([vp, c_i32], c_i32),
+    "fhtgs_server_submit": ([vp, C.POINTER(Request), C.POINTER(C.c_int64)], c_i32),
+    "fhtgs_server_poll": ([vp, C.POINTER(Completion), c_i32, c_i32, C.POINTER(c_i32)], c_i32),
+    "fhtgs_server_release": ([vp, C.c_int64], c_i32),
+    "fhtgs_server_set_paused": ([vp, c_i32], c_i32),
+    "fhtgs_server_drain": ([vp, c_i32], c_i32),
+    "fhtgs_server_get_stats": ([vp, C.POINTER(ServerStats)], c_i32),
+    "fhtgs_server_clock_ms": ([vp], C.c_double),
     "fhtgs_build_tile_masks": ([vp, c_i32, c_i32, vp, vp, vp, vp], c_i32),
     "fhtgs_pack_display": ([C.POINTER(vp), c_i32, c_i32, c_i32, c_i32, c_i32, vp, vp], c_i32),
     "fhtgs_visualize_gaze": ([vp, c_i32, c_i32, c_f, c_f, c_f, c_f, c_f, c_i32, c_i32, c_i32, vp], c_i32),

@@ -8,6 +8,7 @@ Translation units:
   csrc/fhtgs_host.cu    context, arena, orchestration, C ABI (include/fhtgs.h)
   csrc/fhtgs_noalloc.cu the instance sort with a static working array
   csrc/fhtgs_extras.cu  tile-mask builder, display packing, debug overlays
+  csrc/fhtgs_server.cu  request server: resident scenes, continuous batching, HBM admission
 The CUDA runtime is linked statically; the library has no torch dependency.
 """
 from __future__ import annotations
@@ -35,8 +36,9 @@ UNITS = [
     ("fhtgs_host.cu", []),
     ("fhtgs_noalloc.cu", []),
     ("fhtgs_extras.cu", []),
+    ("fhtgs_server.cu", []),
 ]
-HEADERS = ["fhtgs_types.cuh", "fhtgs_math.cuh", "fhtgs_kernels.cuh"]
+HEADERS = ["fhtgs_types.cuh", "fhtgs_math.cuh", "fhtgs_kernels.cuh", "fhtgs_internal.h"]
 
 
 def nvcc() -> str:

@@ -208,6 +208,34 @@ int sort_tiles_for(int64_t cap, int sort_items) {
     return static_cast<int>((cap + tile - 1) / tile);
 }
 
+// Grid sizes of every view of a frame and the arena carve-up it needs at instance capacity `cap`.
+struct FramePlan {
+    std::vector<ViewGeom> geo;
+    int max_tiles = 0, max_large = 0, end_bit = 0, key_u32 = 0, nbp = 0, sort_tiles = 0;
+    Layout L;
+};
+
+FramePlan frame_plan(const fhtgs_primitives* prims, const fhtgs_view* views, int V, const fhtgs_settings* s,
+                     int64_t cap, int sort_items) {
+    FramePlan P;
+    const int64_t N = prims->n_primitives;
+    P.geo.resize(V);
+    for (int i = 0; i < V; ++i) {
+        P.geo[i] = geometry(views[i]);
+        P.max_tiles = std::max(P.max_tiles, P.geo[i].n_tiles);
+        P.max_large = std::max(P.max_large, P.geo[i].n_large);
+        P.end_bit = std::max(P.end_bit, P.geo[i].key_bits);
+    }
+    P.key_u32 = P.max_large > 65536 ? 1 : 0;
+    P.nbp = static_cast<int>((N + kPrimBlock - 1) / kPrimBlock);
+    P.sort_tiles = sort_tiles_for(cap, sort_items);
+    std::vector<int64_t> temp_floats(V, 0);
+    if (s->blur_periphery)
+        for (int i = 0; i < V; ++i) temp_floats[i] = 3ll * views[i].width * views[i].height;
+    P.L = plan(V, N, P.nbp, cap, P.key_u32 ? 4 : 2, P.sort_tiles, P.max_tiles, P.max_large, temp_floats);
+    return P;
+}
+
 // Enqueues one frame on `stream` (no host synchronisation).  `gaze_dev` (null or [n_views][2]
 // floats in device memory) replaces the views' host gaze values at run time.
 fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views, int n_views,
@@ -217,23 +245,13 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     FHTGS_CK(cudaSetDevice(ctx->device));
     const int V = n_views;
     const int64_t N = prims->n_primitives;
-    std::vector<ViewGeom> geo(V);
-    int max_tiles = 0, max_large = 0, end_bit = 0;
-    for (int i = 0; i < V; ++i) {
-        geo[i] = geometry(views[i]);
-        max_tiles = std::max(max_tiles, geo[i].n_tiles);
-        max_large = std::max(max_large, geo[i].n_large);
-        end_bit = std::max(end_bit, geo[i].key_bits);
-    }
     if (ctx->cap <= 0) ctx->cap = estimate_capacity(N);
     const int64_t cap = ctx->cap;
-    const int key_u32 = max_large > 65536 ? 1 : 0;
-    const int nbp = static_cast<int>((N + kPrimBlock - 1) / kPrimBlock);
-    const int sort_tiles = sort_tiles_for(cap, ctx->tuning.sort_items);
-    std::vector<int64_t> temp_floats(V, 0);
-    if (s->blur_periphery)
-        for (int i = 0; i < V; ++i) temp_floats[i] = 3ll * views[i].width * views[i].height;
-    Layout L = plan(V, N, nbp, cap, key_u32 ? 4 : 2, sort_tiles, max_tiles, max_large, temp_floats);
+    FramePlan P = frame_plan(prims, views, V, s, cap, ctx->tuning.sort_items);
+    const std::vector<ViewGeom>& geo = P.geo;
+    const int max_tiles = P.max_tiles, max_large = P.max_large, end_bit = P.end_bit, key_u32 = P.key_u32;
+    const int nbp = P.nbp, sort_tiles = P.sort_tiles;
+    const Layout& L = P.L;
     st = ensure_arena(ctx, L.total);
     if (st != FHTGS_OK) return st;
     char* A = ctx->arena;
@@ -400,6 +418,49 @@ fhtgs_status render_sync_impl(fhtgs_context ctx, const fhtgs_primitives* prims, 
 }
 
 }  // namespace
+
+// Internal interface used by the request server (fhtgs_server.cu), declared in fhtgs_internal.h.
+namespace fhtgs {
+
+fhtgs_status enqueue_frame(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views, int n_views,
+                           const fhtgs_settings* s, cudaStream_t stream, FrameStatus* host_status) {
+    fhtgs_status st = render_impl(ctx, prims, views, n_views, s, stream);
+    if (st != FHTGS_OK || !host_status) return st;
+    FHTGS_CK(cudaMemcpyAsync(host_status, ctx->fb.status, sizeof(FrameStatus) * n_views, cudaMemcpyDeviceToHost, stream));
+    return FHTGS_OK;
+}
+
+size_t frame_arena_need(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views, int n_views,
+                        const fhtgs_settings* s, int64_t cap) {
+    const size_t total = frame_plan(prims, views, n_views, s, cap, ctx->tuning.sort_items).L.total;
+    if (total <= ctx->arena_bytes) return ctx->arena_bytes;
+    return align_up(total + total / 8);  // what ensure_arena allocates
+}
+
+int64_t default_instance_capacity(int64_t n_prims) { return estimate_capacity(n_prims); }
+
+int64_t context_capacity(fhtgs_context ctx) { return ctx->cap; }
+
+void set_context_capacity(fhtgs_context ctx, int64_t cap) {
+    ctx->cap = (std::max<int64_t>(cap, 1) + kSortTile - 1) / kSortTile * kSortTile;
+}
+
+fhtgs_status release_arena(fhtgs_context ctx) {
+    if (!ctx->arena) return FHTGS_OK;
+    FHTGS_CK(cudaSetDevice(ctx->device));
+    FHTGS_CK(cudaFree(ctx->arena));
+    ctx->arena = nullptr;
+    ctx->arena_bytes = 0;
+    ++ctx->arena_generation;
+    ctx->have_frame = false;
+    return FHTGS_OK;
+}
+
+fhtgs_status validate_frame(const fhtgs_primitives* p, const fhtgs_view* views, int n_views, const fhtgs_settings* s) {
+    return validate(p, views, n_views, s);
+}
+
+}  // namespace fhtgs
 
 extern "C" {
 

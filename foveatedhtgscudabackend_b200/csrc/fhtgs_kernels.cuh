@@ -593,6 +593,7 @@ int launch_scan_blocks(const FrameParams& fp, const FrameBuffers& fb, cudaStream
 // reference's touched-tile count)
 // ------------------------------------------------------------------------------------------
 constexpr uint32_t kSeqTiles = 16;   // bounds tiles handled by the owning thread
+constexpr uint32_t kNoPrimitive = 0xFFFFFFFFu;  // value of a sentinel instance slot
 constexpr int kBigList = kPrimBlock;
 
 template <typename KeyT>
@@ -633,6 +634,12 @@ __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParam
                 }
                 ++w;
             }
+            // a visibility area table that counts more tiles than the mask holds leaves slots
+            // over: they get sentinels that the range and blend stages skip
+            for (; w < end && w < lim; ++w) {
+                keys[w] = static_cast<KeyT>(~KeyT(0));
+                vals[w] = kNoPrimitive;
+            }
         } else {
             const uint32_t slot = atomicAdd(&s_big_n, 1u);
             s_big_prim[slot] = static_cast<uint32_t>(i);
@@ -650,6 +657,7 @@ __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParam
         const uint32_t bw = static_cast<uint32_t>(bb.y - bb.x);
         const uint32_t cnt = static_cast<uint32_t>(bb.w - bb.z) * bw;
         uint64_t w0 = s_big_off[q];
+        const uint64_t end = w0 + fb.n_vis[static_cast<size_t>(v) * N + prim];
         for (uint32_t base = 0; base < cnt; base += kPrimBlock) {
             const uint32_t k = base + threadIdx.x;
             uint32_t tile = 0, c = 0;
@@ -660,11 +668,15 @@ __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParam
             uint32_t step;
             const uint32_t ex = block_excl_scan<uint32_t>(c, step, s_warp);
             const uint64_t w = w0 + ex;
-            if (c && w < lim) {
+            if (c && w < lim && w < end) {
                 keys[w] = static_cast<KeyT>(tile);
                 vals[w] = prim;
             }
             w0 += step;
+        }
+        for (uint64_t w = w0 + threadIdx.x; w < end && w < lim; w += kPrimBlock) {  // see above
+            keys[w] = static_cast<KeyT>(~KeyT(0));
+            vals[w] = kNoPrimitive;
         }
     }
 }
@@ -862,19 +874,21 @@ __global__ void __launch_bounds__(256) ranges_kernel(FrameParams fp, FrameBuffer
     const uint64_t M = view_count(fp, fb, v);
     const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[fb.final_buf]) + static_cast<size_t>(v) * fp.cap;
     uint2* r = fb.ranges + static_cast<size_t>(v) * fp.max_large;
+    const uint32_t n_large = static_cast<uint32_t>(fb.views[v].n_large);
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < M;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const KeyT k = keys[i];
+        const bool k_ok = static_cast<uint32_t>(k) < n_large;  // sentinels are no tile
         if (i == 0) {
-            r[k].x = 0;
+            if (k_ok) r[k].x = 0;
         } else {
             const KeyT prev = keys[i - 1];
             if (k != prev) {
-                r[prev].y = static_cast<uint32_t>(i);
-                r[k].x = static_cast<uint32_t>(i);
+                if (static_cast<uint32_t>(prev) < n_large) r[prev].y = static_cast<uint32_t>(i);
+                if (k_ok) r[k].x = static_cast<uint32_t>(i);
             }
         }
-        if (i == M - 1) r[k].y = static_cast<uint32_t>(M);
+        if (i == M - 1 && k_ok) r[k].y = static_cast<uint32_t>(M);
     }
 }
 
@@ -1236,7 +1250,9 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
         for (uint32_t start = range.x; start < range.y; start += NT) {
             const uint32_t n_batch = min(static_cast<uint32_t>(NT), range.y - start);
             __syncthreads();
-            if (static_cast<uint32_t>(tid) < n_batch) {
+            if (static_cast<uint32_t>(tid) < n_batch && vals[start + tid] >= static_cast<uint32_t>(fp.n_prims)) {
+                s_mask[tid] = 0u;  // a sentinel slot: no primitive to blend
+            } else if (static_cast<uint32_t>(tid) < n_batch) {
                 const uint32_t p = vals[start + tid];
                 const float4* r = rec + 4 * static_cast<size_t>(p);
                 const float4 P1 = r[0], P2 = r[1], P4 = r[2], c = r[3];

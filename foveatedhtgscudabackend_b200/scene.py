@@ -232,6 +232,39 @@ def make_batched_views(n_views: int = 64, seed: int = 0, radius=(4.0, 8.0), reso
     return views
 
 
+SERVED_RESOLUTIONS = ((1440, 1584), (2064, 2208))
+
+
+def make_served_requests(duration_s: float, rate_hz: float, n_scenes: int, seed: int = 0,
+                         resolutions=SERVED_RESOLUTIONS, radius=(4.0, 8.0), ipd: float = 0.063,
+                         gaze_sigma: float = 0.1) -> list[tuple[float, int, View, View]]:
+    """A request stream: (arrival s, scene index, left eye, right eye) sorted by arrival.
+
+    Arrivals are Poisson at `rate_hz` over `duration_s`; each request draws its scene uniformly,
+    one resolution (both eyes) uniformly from `resolutions`, a head position uniform on the
+    sphere (away from the poles) at a distance uniform in `radius` looking at the origin, and a
+    gaze of N(0, gaze_sigma) NDC shared by both eyes (eyes at -/+ ipd/2 along the head's x).
+    """
+    rng = np.random.default_rng(seed + 7727)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate_hz)
+        if t >= duration_s:
+            return out
+        si = int(rng.integers(n_scenes))
+        w, h = resolutions[int(rng.integers(len(resolutions)))]
+        while True:
+            d = rng.normal(size=3)
+            d /= np.linalg.norm(d)
+            if abs(d[1]) < 0.95:
+                break
+        pos = tuple(rng.uniform(*radius) * d)
+        g = tuple(np.clip(rng.normal(0.0, gaze_sigma, size=2), -0.95, 0.95))
+        left = make_view(w, h, position=pos, eye_offset=-ipd / 2, gaze_ndc=g)
+        right = make_view(w, h, position=pos, eye_offset=+ipd / 2, gaze_ndc=g)
+        out.append((t, si, left, right))
+
+
 def random_visibility(grid_w: int, grid_h: int, p_visible: float, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
     return rng.random((grid_h, grid_w)) < p_visible

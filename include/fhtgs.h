@@ -284,6 +284,129 @@ fhtgs_status fhtgs_frame_graph_create(fhtgs_context ctx, const fhtgs_primitives*
 fhtgs_status fhtgs_frame_graph_launch(fhtgs_frame_graph graph, void* stream);
 fhtgs_status fhtgs_frame_graph_destroy(fhtgs_frame_graph graph);
 
+/* ---- serving: resident scenes, a request queue and continuous batching ----
+ * No counterpart in the reference, which renders one view (_C) or one stereo pair (_C_stereo)
+ * per blocking call (inference.cu:49-472, inference_stereo.cu:49-828).
+ *
+ * A server owns one scheduler thread and `max_in_flight` frame slots (a context, a stream and
+ * pinned staging each) on one device.  Scenes stay resident: the caller's device arrays are
+ * borrowed until the scene is removed, and their bytes count against the budget.  Requests (one
+ * or two eyes of one scene) are submitted from any host thread and queue up.  Whenever a slot is
+ * free the scheduler takes the oldest queued request together with every other queued request of
+ * the same scene (up to `max_batch_requests`) and renders all their views as ONE frame on that
+ * slot's stream: requests that arrive while others are on the GPU join the next frame of their
+ * scene as soon as a slot frees up, and the frames of different slots overlap on the device.
+ * Nothing in the loop waits for the GPU: a frame's status (instance count) comes back by an
+ * asynchronous copy and its completion by a host function on the slot's stream.  A frame whose
+ * instances overflowed the slot's capacity is rendered again with a larger capacity (its
+ * requests keep their place at the head of the queue).
+ *
+ * Admission: before a frame is launched, the device memory it needs (the slot's arena for its
+ * views and instance capacity, plus server-owned output images) is checked against
+ * `hbm_budget_bytes` together with everything already resident (scenes, the other slots' arenas,
+ * output images, tables).  A frame that does not fit is shrunk to fewer requests; if one request
+ * alone does not fit, idle slots' arenas and unused output buffers are freed, and otherwise the
+ * frame waits until running frames complete.  A request that cannot fit even with nothing else
+ * running fails with FHTGS_ERR_OUT_OF_MEMORY.
+ *
+ * Output: an eye whose `image` is a device pointer is rendered into it (the caller keeps it alive
+ * until the completion); with `image` NULL the server renders into an output buffer of its own
+ * (counted against the budget, recycled) whose address the completion returns; it stays valid
+ * until fhtgs_server_release(ticket).
+ * Results: every view is rendered exactly as fhtgs_render_views renders it alone — a request's
+ * images do not depend on what else shares its frame. */
+typedef struct fhtgs_server_s* fhtgs_server;
+
+typedef struct {
+    int32_t device;
+    int32_t max_in_flight;       /* frame slots, 1..8; 0 = 2                                  */
+    int32_t max_batch_requests;  /* requests fused into one frame, 1..64; 0 = 8                */
+    int32_t reserved;
+    int64_t hbm_budget_bytes;    /* device memory the server may account for; 0 = 150 GB      */
+} fhtgs_server_config;
+
+/* One eye of a request.  The camera values are host floats, copied at submit. */
+typedef struct {
+    float M[12];            /* world -> view, row-major [3,4]                                 */
+    float VPM[16];          /* world -> screen [4,4]                                          */
+    float VPR_inv[16];      /* screen -> world direction [4,4]                                */
+    float cam_position[3];
+    float gaze_x, gaze_y;   /* pixels                                                         */
+    int32_t width, height;
+    float focal_x, focal_y, center_x, center_y;
+    /* device tile tables as in fhtgs_view; NULL visibility mask and area table = every tile
+     * visible (tables built once per resolution by the server); NULL fovea table = the
+     * standard 49x49 table */
+    const uint32_t* visibility_mask;
+    const uint32_t* visibility_mask_area_table;
+    const uint32_t* fovea_mask_area_table;
+    float* image;           /* device output ([3,H,W] or [H,W,3] per the scene's to_chw), or
+                               NULL for a server-owned output buffer                           */
+} fhtgs_eye;
+
+typedef struct {
+    int32_t scene;          /* id from fhtgs_server_add_scene                                 */
+    int32_t n_eyes;         /* 1 or 2                                                         */
+    uint64_t tag;           /* returned unchanged in the completion                           */
+    /* optional cudaEvent_t recorded after the request's device inputs (mask tables, output
+     * images) were produced or last used on the caller's streams; the frame's stream waits
+     * for it.  NULL: those buffers are ready at submit.  Keep the event alive until the
+     * request completes. */
+    void* ready_event;
+    fhtgs_eye eyes[2];
+} fhtgs_request;
+
+typedef struct {
+    int64_t ticket;
+    uint64_t tag;
+    int32_t status;          /* fhtgs_status of this request                                  */
+    int32_t frame_views;     /* views in the frame that rendered it (0 if it never ran)       */
+    double submit_ms;        /* server clock (fhtgs_server_clock_ms) at submit                */
+    double launch_ms;        /* when its (last) frame was enqueued                            */
+    double done_ms;          /* when its frame completed on the GPU                           */
+    float* images[2];        /* device images of the eyes (the caller's or server-owned)      */
+    char message[96];        /* reason of a failure, empty on FHTGS_OK                        */
+} fhtgs_completion;
+
+typedef struct {
+    int64_t submitted, completed, failed;
+    int64_t frames, views, retries;      /* frames launched, views rendered, overflow re-renders */
+    int64_t queued, in_flight;           /* requests waiting / in running frames, right now      */
+    int64_t resident_bytes;              /* accounted against the budget, right now             */
+    int64_t peak_resident_bytes;
+    int64_t admission_waits;             /* times a frame waited for memory to free up          */
+    int64_t max_frame_requests;          /* largest number of requests fused into one frame     */
+} fhtgs_server_stats;
+
+fhtgs_status fhtgs_server_create(const fhtgs_server_config* config, fhtgs_server* out);
+/* Fails queued requests (FHTGS_ERR_NOT_READY), waits for running frames, frees everything the
+ * server allocated.  Completions not yet polled are dropped. */
+fhtgs_status fhtgs_server_destroy(fhtgs_server server);
+/* Registers a resident scene; `prims` (device arrays, complete when this is called: the
+ * server's streams do not wait for the caller's) and `settings` (K, SH bases, planes,
+ * background, to_chw, blur, math) apply to every request of the scene.  Fails with
+ * FHTGS_ERR_OUT_OF_MEMORY if its bytes do not fit the budget beside what is resident. */
+fhtgs_status fhtgs_server_add_scene(fhtgs_server server, const fhtgs_primitives* prims,
+                                    const fhtgs_settings* settings, int32_t* scene_id);
+/* Queued requests of the scene fail; running frames finish; then its bytes leave the budget. */
+fhtgs_status fhtgs_server_remove_scene(fhtgs_server server, int32_t scene_id);
+fhtgs_status fhtgs_server_submit(fhtgs_server server, const fhtgs_request* request, int64_t* ticket);
+/* Moves up to max_completions finished requests (in completion order) into `out`; waits up to
+ * wait_ms for the first one when none is ready. */
+fhtgs_status fhtgs_server_poll(fhtgs_server server, fhtgs_completion* out, int32_t max_completions,
+                               int32_t wait_ms, int32_t* n_out);
+/* Returns the server-owned output buffers of a completed request to the server's pool. */
+fhtgs_status fhtgs_server_release(fhtgs_server server, int64_t ticket);
+/* Paused (1), the server accepts requests but launches no new frame; running frames finish.
+ * Resumed (0), it forms frames from everything queued.  For maintenance windows, and to hand a
+ * whole burst of requests to the batcher at once. */
+fhtgs_status fhtgs_server_set_paused(fhtgs_server server, int32_t paused);
+/* Waits until no request is queued or running (FHTGS_ERR_NOT_READY after timeout_ms; < 0 = no
+ * limit). */
+fhtgs_status fhtgs_server_drain(fhtgs_server server, int32_t timeout_ms);
+fhtgs_status fhtgs_server_get_stats(fhtgs_server server, fhtgs_server_stats* out);
+double fhtgs_server_clock_ms(fhtgs_server server);   /* ms since the server was created */
+
 /* ---- tile masks on the device ----
  * No counterpart in the reference, which takes the three mask tensors precomputed by the
  * calling framework (torch_bindings/rasterization.py:22-43; read at

@@ -53,3 +53,47 @@ def test_library_has_no_torch_or_python_dependency():
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(_lib.FhtgsError):
         _lib.load(str(tmp_path / "nope.so"))
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """ctypes mirrors of the C structs have the header's sizes and field offsets (gcc build)."""
+    structs = {"fhtgs_primitives": _lib.Primitives, "fhtgs_view": _lib.View, "fhtgs_settings": _lib.Settings,
+               "fhtgs_frame_info": _lib.FrameInfo, "fhtgs_intermediates": _lib.Intermediates,
+               "fhtgs_tuning": _lib.Tuning, "fhtgs_server_config": _lib.ServerConfig, "fhtgs_eye": _lib.Eye,
+               "fhtgs_request": _lib.Request, "fhtgs_completion": _lib.Completion,
+               "fhtgs_server_stats": _lib.ServerStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
+    for cname, py in structs.items():
+        ctype = "struct fhtgs_tuning" if cname == "fhtgs_tuning" else cname
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({ctype}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({ctype}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, f"{cname}.{fname}"
+
+
+def test_server_entry_points_fail_cleanly_without_a_device():
+    lib = _lib.load()
+    cfg = _lib.ServerConfig(0, 2, 8, 0, 0)
+    out = _lib.vp()
+    st = lib.fhtgs_server_create(C.byref(cfg), C.byref(out))
+    if st == 0:  # a GPU is present: nothing to check here
+        lib.fhtgs_server_destroy(out)
+        pytest.skip("CUDA device present")
+    assert st in (1, 2) and not out.value
+    assert lib.fhtgs_server_destroy(None) == 0
+    n = C.c_int32(0)
+    assert lib.fhtgs_server_poll(None, None, 1, 0, C.byref(n)) == 1
+    assert lib.fhtgs_server_submit(None, None, None) == 1
+    bad = _lib.ServerConfig(0, 9, 8, 0, 0)
+    assert lib.fhtgs_server_create(C.byref(bad), C.byref(out)) == 1
+    assert b"max_in_flight" in lib.fhtgs_last_error()
