@@ -43,6 +43,30 @@ FP32_LANES_PER_SM = 128
 FLOP_PER_PAIR = 45
 
 
+FOVEATION_TEXT = {
+    "reference": "reference constants: 375 px fovea radius, 125 px blend band, 2x-down periphery",
+    "rings": "rings: full resolution r < {0:g}, 2x down r < {1:g}, 4x down beyond (NDC from the gaze)",
+    "none": "none: every tile at full resolution",
+}
+
+
+def ring_samples(view, mode: str, rings) -> np.ndarray:
+    """Samples blended per large tile (256, 64 or 16) in the ring / no-foveation modes, from the
+    NDC distance of the tile centre to the clamped gaze (the classification of the renderer)."""
+    gw, gh = -(-view.width // 16), -(-view.height // 16)
+    if mode == "none":
+        return np.full(gw * gh, 256, np.int64)
+    f32 = np.float32
+    gx = min(max(f32(view.gaze_position[0]), f32(0)), f32(view.width - 1))
+    gy = min(max(f32(view.gaze_position[1]), f32(0)), f32(view.height - 1))
+    tx, ty = np.meshgrid(np.arange(gw), np.arange(gh))
+    dx = (f32(16) * tx.astype(f32) + f32(8) - gx) / f32(0.5 * view.width)
+    dy = (f32(16) * ty.astype(f32) + f32(8) - gy) / f32(0.5 * view.height)
+    r2 = (dx * dx + dy * dy).astype(f32).reshape(-1)
+    full, half = f32(rings[0]) * f32(rings[0]), f32(rings[1]) * f32(rings[1])
+    return np.where(r2 < full, 256, np.where(r2 < half, 64, 16)).astype(np.int64)
+
+
 def parse(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -68,6 +92,10 @@ def parse(argv=None):
     ap.add_argument("--slots", type=int, default=2, help="frames in flight (served workload)")
     ap.add_argument("--max-batch", type=int, default=8, help="requests per frame (served workload)")
     ap.add_argument("--no-plain", action="store_true", help="served workload: skip the plain per-request path")
+    ap.add_argument("--foveation", choices=["reference", "rings", "none"], default="reference",
+                    help="reference: the reference's fovea/blend/2x layout (comparable with it); rings: full res "
+                         "r < --rings[0], 2x down r < --rings[1], 4x down beyond (NDC); none: all full res")
+    ap.add_argument("--rings", type=float, nargs=2, default=(0.15, 0.4), help="NDC ring radii (rings foveation)")
     return ap.parse_args(argv)
 
 
@@ -159,13 +187,14 @@ def cpu_baseline(g, views, a, budget_s: float) -> dict:
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O  # the CPU baseline leg is the one place bench.py runs the oracle
     cores = os.cpu_count() or 1
+    fov = dict(foveation=a.foveation, rings=tuple(a.rings))
     t_one, _ = O.time_views(g, [views[0]], n_threads=cores, K=a.K, active_sh_bases=(a.sh_degree + 1) ** 2,
-                            precision=32)
+                            precision=32, **fov)
     sample = "one eye (left) of one stereo frame of the benchmark workload"
     total = t_one
     if 2 * t_one <= budget_s:
         t_two, _ = O.time_views(g, [views[1]], n_threads=cores, K=a.K, active_sh_bases=(a.sh_degree + 1) ** 2,
-                                precision=32)
+                                precision=32, **fov)
         total = t_one + t_two
         sample = "one full stereo frame (both eyes) of the benchmark workload"
     else:
@@ -189,6 +218,7 @@ def run_ours(a, world, rank, local):
     gt = F.gaussians_to_torch(g, dev)
     st = [F.settings_from_view(v, K=a.K, active_sh_bases=active, device=dev) for v in (left, right)]
     r = F.Renderer(dev)
+    r.set_foveation(a.foveation, *a.rings)
     imgs = [torch.empty((3, v.height, v.width), device=dev) for v in (left, right)]
 
     # first frame sizes the arena (instance capacity), then warm-up
@@ -226,14 +256,16 @@ def run_ours(a, world, rank, local):
     blend_ms = stage_avg["blend"]
     inter = [r.intermediates(i) for i in range(2)]
     pairs = 0
-    for m in inter:
+    for m, view in zip(inter, (left, right)):
         rng = m["instance_ranges"].astype(np.int64)
         cnt = rng[:, 1] - rng[:, 0]
-        tm = m["tile_index_map_partitioned"]
-        ty = m["tile_type_partitioned"]
-        # 64 pixels per 8x8 sub-tile (fovea, blended) and 64 samples per periphery tile, as the
-        # reference evaluates them
-        pairs += 64 * int(cnt[tm].sum())
+        if a.foveation == "reference":
+            # 64 pixels per 8x8 sub-tile (fovea, blended) and 64 samples per periphery tile, as
+            # the reference evaluates them
+            pairs += 64 * int(cnt[m["tile_index_map_partitioned"]].sum())
+        else:
+            # samples of each large tile at its ring level x the tile's list length
+            pairs += int((ring_samples(view, a.foveation, a.rings) * cnt[0::4]).sum())
     sm_clock = (clk or {}).get("sm_mhz") or 1965.0
     peak_fp32 = torch.cuda.get_device_properties(dev).multi_processor_count * FP32_LANES_PER_SM * 2 * sm_clock * 1e6 / 1e12
     achieved = pairs * FLOP_PER_PAIR / (blend_ms / 1000.0) / 1e12
@@ -262,7 +294,10 @@ def run_ours(a, world, rank, local):
         for s, hi in zip(st, host_in):
             dev_t = {kk: vv.to(dev, non_blocking=True) for kk, vv in hi.items()}
             sd.append(s._replace(**dev_t))
-        a_img, b_img = _C_stereo.render(*gt, *sd[0].as_tuple(), *sd[1].as_tuple(), True, False, False)
+        if a.foveation == "reference":
+            a_img, b_img = _C_stereo.render(*gt, *sd[0].as_tuple(), *sd[1].as_tuple(), True, False, False)
+        else:  # the drop-in call has only the reference's foveation: the Renderer, blocking
+            a_img, b_img = r.render(*gt, sd, to_chw=True, fast_math=True, sync=True)
         buf = k % 2
         copy_done[buf].synchronize()  # the copy that used this pinned buffer two steps ago
         copy_stream.wait_stream(cur)
@@ -288,7 +323,9 @@ def run_ours(a, world, rank, local):
         torch.cuda.synchronize(dev)
         e2e_ms = max_over_ranks(t0.elapsed_time(t1), world)
         e2e = {"value": round(world * e2e_steps / (e2e_ms / 1000.0), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "api": "foveatedhtgscudabackend_b200._C_stereo.render",
+               "d2h_bytes_per_step": int(d2h),
+               "api": "foveatedhtgscudabackend_b200._C_stereo.render" if a.foveation == "reference"
+               else "foveatedhtgscudabackend_b200.Renderer.render (blocking)",
                "steps": e2e_steps, "d2h": "double-buffered pinned copies on a copy stream"}
 
     cpu = None
@@ -302,9 +339,10 @@ def run_ours(a, world, rank, local):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(total_ms_max / a.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_gaussians": a.n_gaussians, "sh_degree": a.sh_degree,
+        "config": {"workload": WORKLOAD + ("" if a.foveation == "reference" else f"_{a.foveation}"),
+                   "n_gaussians": a.n_gaussians, "sh_degree": a.sh_degree,
                    "views": f"2x{a.width}x{a.height}", "K": a.K, "ipd_m": 0.063,
-                   "foveation": "reference constants: 375 px fovea radius, 125 px blend band, 2x-down periphery",
+                   "foveation": FOVEATION_TEXT[a.foveation].format(*a.rings),
                    "math": "fast (matches _C_stereo)", "l2": "inputs larger than L2 (236 MB scene, 2 x 55 MB images)",
                    "parallelism": f"replicated scene, {world} rank(s) x 1 stereo stream"},
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4), "p99": round(float(np.percentile(lat, 99)), 4)},
@@ -313,7 +351,9 @@ def run_ours(a, world, rank, local):
                      "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
                      "frac": round(achieved / peak_fp32, 4), "traffic": None,
                      "peak_source": "nominal FP32 SIMT: SMs x 128 lanes x 2 x median SM clock under load",
-                     "work": f"{pairs} pixel-Gaussian pairs x {FLOP_PER_PAIR} flop (reference's evaluation count)",
+                     "work": f"{pairs} pixel-Gaussian pairs x {FLOP_PER_PAIR} flop "
+                             + ("(reference's evaluation count)" if a.foveation == "reference"
+                                else "(samples of each tile at its ring level x its list length)"),
                      "kernel_ms": round(blend_ms, 4)},
         "stage_ms": {k: round(v, 4) for k, v in stage_avg.items()},
         "instances_per_eye": [int(i["n_instances"]) for i in info],
@@ -518,7 +558,8 @@ def run_served(a, world, rank, local):
     n_req = len(trace)
 
     srv = Server(dev, hbm_budget_bytes=150e9, max_in_flight=a.slots, max_batch_requests=a.max_batch)
-    ids = [srv.add_scene(*gt, K=a.K, active_sh_bases=active) for gt in scenes]
+    ids = [srv.add_scene(*gt, K=a.K, active_sh_bases=active, foveation=a.foveation, rings=tuple(a.rings))
+           for gt in scenes]
 
     def drain_all(expect):
         got = 0
@@ -589,11 +630,20 @@ def run_served(a, world, rank, local):
     pct = lambda x, q: round(float(np.percentile(x, q)), 3)
     plain = None
     if not a.no_plain:
+        if a.foveation == "reference":
+            def plain_call(si, sd):
+                return _C_stereo.render(*scenes[si], *sd[0].as_tuple(), *sd[1].as_tuple(), True, False, False)
+        else:  # the drop-in call has only the reference's foveation: a blocking Renderer call
+            rp = F.Renderer(dev)
+            rp.set_foveation(a.foveation, *a.rings)
+
+            def plain_call(si, sd):
+                return rp.render(*scenes[si], sd, to_chw=True, fast_math=True, sync=True)
         sts = [[F.settings_from_view(v, K=a.K, active_sh_bases=active, device=dev) for v in (l, r)]
                for t, si, l, r in trace]
         for t, si, l, r in warm[:6]:
             w = [F.settings_from_view(v, K=a.K, active_sh_bases=active, device=dev) for v in (l, r)]
-            _C_stereo.render(*scenes[si], *w[0].as_tuple(), *w[1].as_tuple(), True, False, False)
+            plain_call(si, w)
         torch.cuda.synchronize(dev)
         clock = time.perf_counter
         t0p = 1000.0 * clock() + 20.0
@@ -602,14 +652,15 @@ def run_served(a, world, rank, local):
             arr = t0p + 1000.0 * t
             while 1000.0 * clock() < arr:
                 pass
-            _C_stereo.render(*scenes[si], *sts[k][0].as_tuple(), *sts[k][1].as_tuple(), True, False, False)
+            plain_call(si, sts[k])
             lat_p.append(1000.0 * clock() - arr)
         plain_s = (1000.0 * clock() - t0p) / 1000.0
         ts = clock()
         for k, (t, si, l, r) in enumerate(trace):
-            _C_stereo.render(*scenes[si], *sts[k][0].as_tuple(), *sts[k][1].as_tuple(), True, False, False)
+            plain_call(si, sts[k])
         plain_sat = n_req / (clock() - ts)
-        plain = {"api": "foveatedhtgscudabackend_b200._C_stereo.render, one blocking call per request",
+        plain = {"api": ("foveatedhtgscudabackend_b200._C_stereo.render" if a.foveation == "reference"
+                         else "foveatedhtgscudabackend_b200.Renderer.render (blocking)") + ", one call per request",
                  "requests_per_s": round(n_req / plain_s, 2), "p50_ms": pct(lat_p, 50), "p99_ms": pct(lat_p, 99),
                  "max_ms": round(max(lat_p), 3), "saturated_requests_per_s": round(plain_sat, 2)}
 
@@ -620,7 +671,9 @@ def run_served(a, world, rank, local):
         "value": round(n_req / served_s, 2), "unit": "requests/s", "n_gpus": world, "steps": n_req, "warmup": 2 * len(warm),
         "ms_per_step": round(1000.0 * served_s / n_req, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"served_{'_'.join(str(n // 1000) + 'k' for n in SERVED_SCENES)}_sh{a.sh_degree}_poisson{a.rate:g}",
+        "config": {"workload": f"served_{'_'.join(str(n // 1000) + 'k' for n in SERVED_SCENES)}_sh{a.sh_degree}_poisson{a.rate:g}"
+                               + ("" if a.foveation == "reference" else f"_{a.foveation}"),
+                   "foveation": FOVEATION_TEXT[a.foveation].format(*a.rings),
                    "scenes": list(SERVED_SCENES), "rate_per_s": a.rate, "duration_s": a.duration, "requests": n_req,
                    "resolutions_per_eye": "uniform from 1440x1584, 2064x2208", "K": a.K,
                    "head_pose": "sphere r in [4, 8] looking at the origin; gaze N(0, 0.1) NDC",

@@ -59,7 +59,11 @@ class Settings(C.Structure):
     _fields_ = [("K", c_i32), ("active_sh_bases", c_i32), ("near_plane", c_f), ("far_plane", c_f),
                 ("scale_modifier", c_f), ("to_chw", c_i32), ("blur_periphery", c_i32), ("anti_aliasing", c_i32),
                 ("background_type", c_i32), ("background_data", vp), ("texture_width", c_i32),
-                ("texture_height", c_i32), ("fast_math", c_i32)]
+                ("texture_height", c_i32), ("fast_math", c_i32), ("foveation", c_i32), ("ring_full", c_f),
+                ("ring_half", c_f)]
+
+
+FOVEATION = {"reference": 0, "rings": 1, "none": 2}
 
 
 class FrameInfo(C.Structure):

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -182,6 +183,13 @@ fhtgs_status validate(const fhtgs_primitives* p, const fhtgs_view* views, int n_
     if (s->background_type != 0 && !s->background_data) return fail(FHTGS_ERR_INVALID_ARGUMENT, "background data is null");
     if ((s->background_type == 2 || s->background_type == 3) && (s->texture_width <= 0 || s->texture_height <= 0))
         return fail(FHTGS_ERR_INVALID_ARGUMENT, "texture background needs positive texture size");
+    if (s->foveation < FHTGS_FOVEATION_REFERENCE || s->foveation > FHTGS_FOVEATION_NONE)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "unknown foveation mode");
+    if (s->foveation == FHTGS_FOVEATION_RINGS) {
+        if (!(s->ring_full >= 0.0f) || !(s->ring_half >= s->ring_full) || !std::isfinite(s->ring_half))
+            return fail(FHTGS_ERR_INVALID_ARGUMENT, "ring radii must satisfy 0 <= ring_full <= ring_half < inf");
+        if (s->blur_periphery) return fail(FHTGS_ERR_INVALID_ARGUMENT, "blur_periphery is not available with ring foveation");
+    }
     for (int i = 0; i < n_views; ++i) {
         const fhtgs_view& v = views[i];
         if (v.width <= 0 || v.height <= 0) return fail(FHTGS_ERR_INVALID_ARGUMENT, "view size must be positive");
@@ -280,6 +288,9 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     fp.n_blocks_prim = nbp;
     fp.blend_rw = ctx->tuning.blend_warp_width;
     fp.blend_blocks = ctx->tuning.blend_blocks_per_sm;
+    fp.fov_mode = s->foveation;
+    fp.ring_full2 = s->ring_full * s->ring_full;
+    fp.ring_half2 = s->ring_half * s->ring_half;
 
     FrameBuffers fb{};
     fb.views = reinterpret_cast<ViewParams*>(A + L.off_views);
@@ -570,7 +581,8 @@ fhtgs_status fhtgs_get_frame_info(fhtgs_context ctx, int32_t view, fhtgs_frame_i
     fhtgs_status st = read_status(ctx);
     if (st != FHTGS_OK) return st;
     const FrameStatus& s = ctx->h_status[view];
-    out->n_instances = static_cast<int64_t>(s.n_instances_ref);
+    // the reference's count has a meaning only in its own foveation layout
+    out->n_instances = static_cast<int64_t>(ctx->fp.fov_mode == kFoveationReference ? s.n_instances_ref : s.n_instances);
     out->instance_capacity = ctx->fp.cap;
     out->n_active_tiles = s.n_active;
     for (int k = 0; k < 6; ++k) out->partition_ranges[k] = s.ranges[k];
@@ -625,7 +637,10 @@ fhtgs_status fhtgs_copy_intermediates(fhtgs_context ctx, int32_t view, fhtgs_int
     // keys are small-tile ids 4*t+i, the list of a fovea-circle tile (type fovea or blended) is
     // repeated for its four sub-tiles, other visible tiles carry key 4*t once; the slots its
     // area tables over-count follow as sentinel keys, up to its instance count.
-    const uint64_t m_ref = s.n_instances_ref;
+    // Other foveation modes have no reference layout: each stored list appears once, keyed by
+    // its large tile's first sub-tile, without sentinel slots.
+    const bool ref_layout = fp.fov_mode == kFoveationReference;
+    const uint64_t m_ref = ref_layout ? s.n_instances_ref : Ms;
     const uint32_t sentinel = g.end_bit <= 16 ? 0xFFFFu : 0xFFFFFFFFu;
     uint64_t pos = 0;
     std::vector<uint2> rr(T, make_uint2(0, 0));
@@ -633,7 +648,7 @@ fhtgs_status fhtgs_copy_intermediates(fhtgs_context ctx, int32_t view, fhtgs_int
         const uint2 r = lr[t];
         if (r.y <= r.x) continue;
         const uint32_t len = r.y - r.x;
-        const int reps = (lt[t] == kFovea || lt[t] == kBlended) ? kSubTiles : 1;
+        const int reps = ref_layout && (lt[t] == kFovea || lt[t] == kBlended) ? kSubTiles : 1;
         for (int i = 0; i < reps; ++i) {
             const uint32_t key = static_cast<uint32_t>(t) * kSubTiles + i;
             if (pos + len > m_ref) return fail(FHTGS_ERR_CAPACITY, "stored instances exceed the reference count");

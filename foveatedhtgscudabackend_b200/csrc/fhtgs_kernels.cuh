@@ -135,9 +135,24 @@ int launch_setup(const ViewSetup* setups, int n_views, ViewParams* out, cudaStre
 // build_tile_index_map, the 2-bit type sort and get_partition_ranges_cu of the reference,
 // shared_kernels.cuh:155-238, inference.cu:131-188, with one block per view)
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ uint8_t large_tile_type(const ViewParams& vp, uint32_t tile) {
+// Ring level of a large tile: squared NDC distance of the tile centre from the (clamped) gaze,
+// x and y each scaled by half the image size, in explicitly rounded IEEE steps (the CPU
+// oracle evaluates the same sequence, so both agree on every tile).
+__device__ __forceinline__ uint8_t ring_tile_type(const ViewParams& vp, const FrameParams& fp, uint32_t tx,
+                                                  uint32_t ty) {
+    const float cx = static_cast<float>(tx * kTileLarge + kTileLarge / 2);
+    const float cy = static_cast<float>(ty * kTileLarge + kTileLarge / 2);
+    const float dx = __fdiv_rn(__fsub_rn(cx, vp.gaze_px.x), __fmul_rn(0.5f, static_cast<float>(vp.width)));
+    const float dy = __fdiv_rn(__fsub_rn(cy, vp.gaze_px.y), __fmul_rn(0.5f, static_cast<float>(vp.height)));
+    const float r2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+    return r2 < fp.ring_full2 ? kFovea : r2 < fp.ring_half2 ? kPeriphery : kQuarter;
+}
+
+__device__ __forceinline__ uint8_t large_tile_type(const ViewParams& vp, const FrameParams& fp, uint32_t tile) {
     if (!tile_visible(vp.vis_mask, tile)) return kMasked;
+    if (fp.fov_mode == kFoveationNone) return kFovea;
     const uint32_t tx = tile % static_cast<uint32_t>(vp.glw), ty = tile / static_cast<uint32_t>(vp.glw);
+    if (fp.fov_mode == kFoveationRings) return ring_tile_type(vp, fp, tx, ty);
     if (in_fovea<kFoveaRadiusTiles>(tx, ty, vp.gaze_tiles))
         return in_fovea<kBlendRadiusTiles>(tx, ty, vp.gaze_tiles) ? kFovea : kBlended;
     return kPeriphery;
@@ -150,21 +165,26 @@ __global__ void __launch_bounds__(1024) classify_kernel(FrameParams fp, FrameBuf
     const int TL = vp.n_large;
     const int seg = (TL + blockDim.x - 1) / blockDim.x;
     const int b0 = min(TL, static_cast<int>(threadIdx.x) * seg), b1 = min(TL, b0 + seg);
-    uint32_t cnt[4] = {0, 0, 0, 0};
-    for (int t = b0; t < b1; ++t) cnt[large_tile_type(vp, t)]++;
-    // two packed 64-bit scans: (fovea | periphery << 32), (blended | masked << 32)
-    unsigned long long tot0, tot1;
+    uint32_t cnt[5] = {0, 0, 0, 0, 0};
+    for (int t = b0; t < b1; ++t) cnt[large_tile_type(vp, fp, t)]++;
+    // packed 64-bit scans: (fovea | periphery << 32), (blended | masked << 32), quarter
+    unsigned long long tot0, tot1, tot2;
     unsigned long long e0 = block_excl_scan<unsigned long long>(cnt[0] | (static_cast<unsigned long long>(cnt[1]) << 32), tot0, s_warp);
     unsigned long long e1 = block_excl_scan<unsigned long long>(cnt[2] | (static_cast<unsigned long long>(cnt[3]) << 32), tot1, s_warp);
+    unsigned long long e2 = block_excl_scan<unsigned long long>(cnt[4], tot2, s_warp);
     const uint32_t nF = static_cast<uint32_t>(tot0), nP = static_cast<uint32_t>(tot0 >> 32);
     const uint32_t nB = static_cast<uint32_t>(tot1), nM = static_cast<uint32_t>(tot1 >> 32);
+    const uint32_t nQ = static_cast<uint32_t>(tot2);
     uint32_t oF = static_cast<uint32_t>(e0), oP = static_cast<uint32_t>(e0 >> 32);
     uint32_t oB = static_cast<uint32_t>(e1), oM = static_cast<uint32_t>(e1 >> 32);
-    const uint32_t n_active = kSubTiles * nF + nP + kSubTiles * nB;
+    uint32_t oQ = static_cast<uint32_t>(e2);
+    // quarter tiles appear in the partitioned map as periphery entries (after the others)
+    const uint32_t n_active = kSubTiles * nF + nP + nQ + kSubTiles * nB;
     // The reference renders nothing when exactly one small-tile entry is active (its
     // partition-range kernel starts at index 1, shared_kernels.cuh:222-238); that tile is then
-    // cleared instead of blended, which matches the zero-initialised output of _C.
-    const bool none = n_active <= 1;
+    // cleared instead of blended, which matches the zero-initialised output of _C.  The other
+    // foveation modes have no counterpart there and no such rule.
+    const bool none = fp.fov_mode == kFoveationReference && n_active <= 1;
     uint32_t* map = fb.tile_map_part + static_cast<size_t>(v) * fp.max_tiles;
     uint8_t* typ = fb.tile_type_part + static_cast<size_t>(v) * fp.max_tiles;
     uint8_t* lt = fb.large_type + static_cast<size_t>(v) * fp.max_large;
@@ -172,7 +192,7 @@ __global__ void __launch_bounds__(1024) classify_kernel(FrameParams fp, FrameBuf
     uint32_t* wl = fb.work_low + static_cast<size_t>(v) * fp.max_large;
     uint32_t* wm = fb.work_masked + static_cast<size_t>(v) * fp.max_large;
     for (int t = b0; t < b1; ++t) {
-        const uint8_t ty = large_tile_type(vp, t);
+        const uint8_t ty = large_tile_type(vp, fp, t);
         lt[t] = ty;
         const uint32_t sub0 = static_cast<uint32_t>(t) * kSubTiles;
         if (ty == kFovea) {
@@ -183,9 +203,12 @@ __global__ void __launch_bounds__(1024) classify_kernel(FrameParams fp, FrameBuf
             if (none) wm[nM] = t; else wl[oP] = t;
             ++oP;
         } else if (ty == kBlended) {
-            const uint32_t base = kSubTiles * nF + nP + kSubTiles * oB;
+            const uint32_t base = kSubTiles * nF + nP + nQ + kSubTiles * oB;
             for (int i = 0; i < kSubTiles; ++i) { map[base + i] = sub0 + i; typ[base + i] = kBlended; }
             wf[nF + oB++] = t;
+        } else if (ty == kQuarter) {
+            map[kSubTiles * nF + nP + oQ] = sub0; typ[kSubTiles * nF + nP + oQ] = kPeriphery;
+            wl[nP + oQ++] = t;
         } else {
             wm[oM++] = t;
         }
@@ -196,12 +219,13 @@ __global__ void __launch_bounds__(1024) classify_kernel(FrameParams fp, FrameBuf
         for (int k = 0; k < 6; ++k) st.ranges[k] = 0;
         if (!none) {
             if (nF) { st.ranges[0] = 0; st.ranges[1] = kSubTiles * nF; }
-            if (nP) { st.ranges[2] = kSubTiles * nF; st.ranges[3] = kSubTiles * nF + nP; }
-            if (nB) { st.ranges[4] = kSubTiles * nF + nP; st.ranges[5] = n_active; }
+            if (nP + nQ) { st.ranges[2] = kSubTiles * nF; st.ranges[3] = kSubTiles * nF + nP + nQ; }
+            if (nB) { st.ranges[4] = kSubTiles * nF + nP + nQ; st.ranges[5] = n_active; }
         }
         st.n_fovea_large = nF;
         st.n_blended_large = nB;
         st.n_periphery_large = none ? 0 : nP;
+        st.n_quarter_large = nQ;
         st.n_masked_large = none ? nM + nP : nM;
         st.overflow = 0;
         st.n_instances = 0;
@@ -914,7 +938,7 @@ int launch_ranges(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cuda
 constexpr uint32_t kItemLowres = 1u << 23;
 
 __device__ __forceinline__ int items_of_view(const FrameStatus& st) {
-    return static_cast<int>(st.n_fovea_large + st.n_blended_large + st.n_periphery_large);
+    return static_cast<int>(st.n_fovea_large + st.n_blended_large + st.n_periphery_large + st.n_quarter_large);
 }
 
 __device__ __forceinline__ int cost_bucket(uint32_t cost) {
@@ -945,7 +969,8 @@ __device__ __forceinline__ uint32_t item_cost(const FrameParams& fp, const Frame
     const uint2 r = fb.ranges[static_cast<size_t>(v) * fp.max_large + lt];
     packed = (static_cast<uint32_t>(v) << 24) | (low ? kItemLowres : 0u) | static_cast<uint32_t>(idx);
     const uint32_t len = r.y > r.x ? r.y - r.x : 0u;
-    return len * (low ? 2u : 8u);
+    const bool quarter = low && static_cast<uint32_t>(idx) >= st.n_periphery_large;
+    return len * (quarter ? 1u : low ? 2u : 8u);
 }
 
 constexpr int kMaxOrderViews = 1024;
@@ -1221,20 +1246,24 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
         const uint32_t lt = low ? fb.work_low[static_cast<size_t>(v) * fp.max_large + item]
                                 : fb.work_full[static_cast<size_t>(v) * fp.max_large + item];
         const bool is_fovea = !low && static_cast<uint32_t>(item) < st.n_fovea_large;
-        const int S = low ? kStride : 1;
+        // ring mode: the quarter tiles follow the periphery tiles in work_low (4 x 4 samples
+        // at stride 4, lanes 0-15 of warp 0)
+        const bool quarter = low && static_cast<uint32_t>(item) >= st.n_periphery_large;
+        const int S = quarter ? kQuarterStride : low ? kStride : 1;
         // warp rectangle rw x rh (powers of two); warps laid out 2^wx_bits per row
         constexpr int RW_LOW = RW > 8 ? 8 : RW;  // the periphery sample grid is 8 wide
         constexpr int RW_BITS = RW == 4 ? 2 : RW == 8 ? 3 : 4, RW_LOW_BITS = RW_LOW == 4 ? 2 : 3;
-        const int rw_bits = low ? RW_LOW_BITS : RW_BITS;
+        const int rw_bits = quarter ? 2 : low ? RW_LOW_BITS : RW_BITS;
         const int rw = 1 << rw_bits, rh = 32 >> rw_bits;
-        const int wx_bits = (low ? 3 : 4) - rw_bits;
-        const int n_warps = low ? 2 : NW;
+        const int rh_used = quarter ? 4 : rh;  // sample rows of a warp that lie in the tile
+        const int wx_bits = quarter ? 0 : (low ? 3 : 4) - rw_bits;
+        const int n_warps = quarter ? 1 : low ? 2 : NW;
         const int ox = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)) * kTileLarge;
         const int oy = static_cast<int>(lt / static_cast<uint32_t>(vp.glw)) * kTileLarge;
         const int lx = (warp & ((1 << wx_bits) - 1)) * rw + (lane & (rw - 1));
         const int ly = (warp >> wx_bits) * rh + (lane >> rw_bits);
         const int px_i = ox + lx * S, py_i = oy + ly * S;
-        const bool inside = warp < n_warps && px_i < vp.width && py_i < vp.height;
+        const bool inside = warp < n_warps && (lane >> rw_bits) < rh_used && px_i < vp.width && py_i < vp.height;
         const float pixel_x = __uint2float_rn(static_cast<uint32_t>(px_i));
         const float pixel_y = __uint2float_rn(static_cast<uint32_t>(py_i));
         const uint2 range = fb.ranges[static_cast<size_t>(v) * fp.max_large + lt];
@@ -1273,7 +1302,7 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
                             const float ax0 = static_cast<float>(ox + (w & ((1 << wx_bits) - 1)) * rw * S);
                             const float ax1 = ax0 + static_cast<float>((rw - 1) * S);
                             const float ay0 = static_cast<float>(oy + (w >> wx_bits) * rh * S);
-                            const float ay1 = ay0 + static_cast<float>((rh - 1) * S);
+                            const float ay1 = ay0 + static_cast<float>((rh_used - 1) * S);
                             if (box.y >= ax0 && box.x <= ax1 && box.w >= ay0 && box.z <= ay1 &&
                                 (!ell || conic_meets_rect(q, ax0, ax1, ay0, ay1)))
                                 m |= 1u << w;
@@ -1414,7 +1443,8 @@ __device__ __forceinline__ float3 grid_sample(const ViewParams& vp, const uint8_
     const int px = bx + min(sx, max_r) * kStride;
     const int py = by + min(sy, max_d) * kStride;
     const int tile = py / kTileLarge * vp.glw + px / kTileLarge;
-    if ((vp.vis_mask[tile / 32] & (1u << (tile % 32))) == 0) {
+    // a quarter tile (ring mode) holds no stride-2 samples: treated like a masked neighbour
+    if ((vp.vis_mask[tile / 32] & (1u << (tile % 32))) == 0 || ltype[tile] == kQuarter) {
         const int cx = clampi(px, ltx * kTileLarge, ltx * kTileLarge + kTileLarge - kStride);
         const int cy = clampi(py, lty * kTileLarge, lty * kTileLarge + kTileLarge - kStride);
         return load_rgb(src, vp.width, vp.height, cx, cy, chw);
@@ -1426,15 +1456,34 @@ __device__ __forceinline__ float3 grid_sample(const ViewParams& vp, const uint8_
     return load_rgb(src, vp.width, vp.height, px, py, chw);
 }
 
+// Sample (sx, sy) of the stride-4 grid of a quarter tile (ring mode) starting at its origin
+// (ox, oy): every visible tile holds the stride-4 positions (full, 2x and 4x tiles alike);
+// samples in masked tiles are clamped into the tile (ltx, lty), as the periphery grid is.
+__device__ __forceinline__ float3 grid_sample4(const ViewParams& vp, const float* src, bool chw, int ox, int oy,
+                                               int sx, int sy, int max_r, int max_d, int ltx, int lty) {
+    const int px = ox + min(sx, max_r) * kQuarterStride;
+    const int py = oy + min(sy, max_d) * kQuarterStride;
+    const int tile = py / kTileLarge * vp.glw + px / kTileLarge;
+    if ((vp.vis_mask[tile / 32] & (1u << (tile % 32))) == 0) {
+        const int cx = clampi(px, ltx * kTileLarge, ltx * kTileLarge + kTileLarge - kQuarterStride);
+        const int cy = clampi(py, lty * kTileLarge, lty * kTileLarge + kTileLarge - kQuarterStride);
+        return load_rgb(src, vp.width, vp.height, cx, cy, chw);
+    }
+    return load_rgb(src, vp.width, vp.height, px, py, chw);
+}
+
+// Bilinear fill between the samples of an S-strided grid (S = 2: the reference's periphery
+// interpolation; S = 4: the ring mode's quarter tiles, same steps).
+template <int S = kStride>
 __device__ __forceinline__ float3 bilerp(const float3* s, int n, int lx, int ly) {
-    const int bx = lx / kStride, by = ly / kStride;
-    const float xf = static_cast<float>(lx % kStride) / static_cast<float>(kStride);
-    const float yf = static_cast<float>(ly % kStride) / static_cast<float>(kStride);
+    const int bx = lx / S, by = ly / S;
+    const float xf = static_cast<float>(lx % S) / static_cast<float>(S);
+    const float yf = static_cast<float>(ly % S) / static_cast<float>(S);
     float3 r = make_float3(0.0f, 0.0f, 0.0f);
-    if (lx % kStride == 0) {
+    if (lx % S == 0) {
         r += s[by * n + bx] * (1.0f - yf);
         r += s[(by + 1) * n + bx] * yf;
-    } else if (ly % kStride == 0) {
+    } else if (ly % S == 0) {
         r += s[by * n + bx] * (1.0f - xf);
         r += s[by * n + bx + 1] * xf;
     } else {
@@ -1477,9 +1526,9 @@ __global__ void __launch_bounds__(256) compose_kernel(FrameParams fp, FrameBuffe
     const ViewParams& vp = fb.views[v];
     const FrameStatus& st = fb.status[v];
     const int nP = static_cast<int>(st.n_periphery_large), nB = static_cast<int>(st.n_blended_large),
-              nM = static_cast<int>(st.n_masked_large);
+              nM = static_cast<int>(st.n_masked_large), nQ = static_cast<int>(st.n_quarter_large);
     int item = blockIdx.x;
-    if (item >= nP + nB + nM) return;
+    if (item >= nP + nQ + nB + nM) return;
     const bool chw = fp.to_chw != 0;
     const bool blur = fp.blur != 0;
     const float* src = vp.work;
@@ -1514,6 +1563,26 @@ __global__ void __launch_bounds__(256) compose_kernel(FrameParams fp, FrameBuffe
         return;
     }
     item -= nP;
+    if (item < nQ) {
+        // ring mode: 4x-down tile, 5 x 5 samples at stride 4 (its own 4 x 4 and the first
+        // row/column of its right and lower neighbours)
+        const uint32_t lt = fb.work_low[static_cast<size_t>(v) * fp.max_large + nP + item];
+        const int ltx = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)), lty = static_cast<int>(lt / static_cast<uint32_t>(vp.glw));
+        const int ox = ltx * kTileLarge, oy = lty * kTileLarge;
+        const int max_r = static_cast<int>((static_cast<unsigned>(W) - static_cast<unsigned>(ox) - 1u) / static_cast<unsigned>(kQuarterStride));
+        const int max_d = static_cast<int>((static_cast<unsigned>(H) - static_cast<unsigned>(oy) - 1u) / static_cast<unsigned>(kQuarterStride));
+        float3* s = s_samples[0];
+        if (tid < 25) s[tid] = grid_sample4(vp, src, chw, ox, oy, tid % 5, tid / 5, max_r, max_d, ltx, lty);
+        __syncthreads();
+        const int lx = tid & 15, ly = tid >> 4;
+        const int px = ox + lx, py = oy + ly;
+        if (px >= W || py >= H) return;
+        if ((lx % kQuarterStride) == 0 && (ly % kQuarterStride) == 0) return;
+        const float3 r = bilerp<kQuarterStride>(s, 5, lx, ly);
+        store_rgb(dst, W, H, px, py, chw, __saturatef(r.x), __saturatef(r.y), __saturatef(r.z));
+        return;
+    }
+    item -= nQ;
     if (item < nB) {
         const uint32_t lt = fb.work_full[static_cast<size_t>(v) * fp.max_large + st.n_fovea_large + item];
         const int ltx = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)), lty = static_cast<int>(lt / static_cast<uint32_t>(vp.glw));

@@ -25,7 +25,13 @@ constexpr int kBlendRadiusTiles = (kFoveaRadiusPx - kBlendWidthPx) / kTileLarge;
 constexpr int kBlendRadiusPx = kBlendRadiusTiles * kTileLarge;                     // 240
 constexpr int kFoveaTableSide = 2 * kFoveaRadiusTiles + 1;                         // 49
 
-enum TileType : uint8_t { kFovea = 0, kPeriphery = 1, kBlended = 2, kMasked = 3 };
+// kQuarter exists only in the ring foveation mode (tiles sampled at stride 4).
+enum TileType : uint8_t { kFovea = 0, kPeriphery = 1, kBlended = 2, kMasked = 3, kQuarter = 4 };
+constexpr int kQuarterStride = 4;
+
+// Foveation modes (fhtgs_settings.foveation): the reference's fixed fovea/blend/periphery
+// tiles; rings by NDC distance from the gaze (full / 2x down / 4x down); none (all full).
+enum FoveationMode : int { kFoveationReference = 0, kFoveationRings = 1, kFoveationNone = 2 };
 
 // Per-view parameters, resident in device memory for the whole frame (filled by the
 // setup kernel from the caller's device matrices and host scalars).
@@ -78,6 +84,9 @@ struct FrameParams {
     int n_blocks_prim;     // preprocess/create blocks per view
     int blend_rw;          // blend: pixels per warp row (4, 8 or 16; 32 / blend_rw rows)
     int blend_blocks;      // persistent blend blocks per SM (0: as many as fit)
+    int fov_mode;          // FoveationMode
+    float ring_full2;      // rings: squared NDC radius of full resolution
+    float ring_half2;      // rings: squared NDC radius of 2x-down sampling (4x beyond)
 };
 
 // Per-view frame status written by the device, read by the host after the frame.
@@ -91,7 +100,8 @@ struct FrameStatus {
     uint32_t ranges[6];               // partition ranges (fovea, periphery, blended)
     uint32_t n_fovea_large, n_blended_large, n_periphery_large, n_masked_large;
     uint32_t overflow;
-    uint32_t pad;
+    uint32_t n_quarter_large;         // ring mode: tiles sampled at stride 4 (after the
+                                      // periphery tiles in work_low)
 };
 
 // Attribute arrays; with `half` set, scales/rotations/opacities hold fp16 and sh_0/sh_rest
@@ -128,7 +138,7 @@ struct FrameBuffers {
     uint8_t* tile_type_part;  // [V][max_tiles]
     uint8_t* large_type;      // [V][max_large]
     uint32_t* work_full;      // [V][max_large] fovea then blended large tiles
-    uint32_t* work_low;       // [V][max_large] periphery large tiles
+    uint32_t* work_low;       // [V][max_large] periphery large tiles, then quarter tiles
     uint32_t* work_masked;    // [V][max_large] masked large tiles
     uint32_t* counters;       // [kCounterWords]: work counters, then the work-order buckets
     uint32_t* work_order[2];  // [0]: [V*max_large] packed blend items, heaviest first; [1] unused

@@ -296,6 +296,7 @@ class Renderer:
         self.ctx = out.value
         self._last_views = 0
         self._last_n = 0
+        self._foveation = (0, 0.0, 0.0)
 
     def close(self):
         if getattr(self, "ctx", None):
@@ -307,6 +308,15 @@ class Renderer:
             self.close()
         except Exception:
             pass
+
+    def set_foveation(self, mode: str = "reference", ring_full: float = 0.15, ring_half: float = 0.4):
+        """Foveation of this renderer's frames (fhtgs_settings.foveation): "reference" (the
+        reference's fixed fovea / blend band / 2x periphery, the default), "rings" (full
+        resolution within NDC radius ring_full of the gaze, 2x down within ring_half, 4x down
+        beyond) or "none" (every tile at full resolution)."""
+        if mode not in _lib.FOVEATION:
+            raise ValueError(f"foveation must be one of {sorted(_lib.FOVEATION)}")
+        self._foveation = (_lib.FOVEATION[mode], float(ring_full), float(ring_half))
 
     def reserve(self, n_primitives: int, n_views: int, max_width: int, max_height: int, instances_per_view: int = 0):
         _lib.check(self._libh.fhtgs_context_reserve(self.ctx, n_primitives, n_views, max_width, max_height,
@@ -361,7 +371,7 @@ class Renderer:
         st = _lib.Settings(int(s0.K), int(s0.active_sh_bases), float(s0.near_plane), float(s0.far_plane),
                            float(s0.scale_modifier), int(bool(to_chw)), int(bool(blur_periphery)), int(bool(aaa_mode)),
                            bg_type, keep.f32(s0.background_model_data, "background_model_data"), tw, th,
-                           int(bool(fast_math)))
+                           int(bool(fast_math)), *self._foveation)
         if images is None:
             images = [_alloc_image(to_chw, int(s.height), int(s.width), dev) for s in settings]
         views = (_lib.View * len(settings))()

@@ -130,8 +130,12 @@ class Server:
                   active_sh_bases: int = 16, near_plane: float = 0.2, far_plane: float = 100.0,
                   scale_modifier: float = 1.0, to_chw: bool = True, blur_periphery: bool = False,
                   aaa_mode: bool = False, fast_math: bool = True, background: BackgroundModel = BackgroundModel.NONE,
-                  background_data: torch.Tensor | None = None) -> int:
-        """Registers resident Gaussians (device tensors, fp32 or the fp16/bf16 storage)."""
+                  background_data: torch.Tensor | None = None, foveation: str = "reference",
+                  rings: tuple[float, float] = (0.15, 0.4)) -> int:
+        """Registers resident Gaussians (device tensors, fp32 or the fp16/bf16 storage).
+        `foveation` / `rings`: as Renderer.set_foveation, for every request of the scene."""
+        if foveation not in _lib.FOVEATION:
+            raise ValueError(f"foveation must be one of {sorted(_lib.FOVEATION)}")
         keep = _Keep(self.device)
         n, total_sh = _check_gaussians(positions, scales, rotations, opacities, sh_0, sh_rest)
         # the server's streams do not wait for PyTorch's: the scene must be complete now
@@ -153,7 +157,8 @@ class Server:
         tw, th = _texture_size(bg_type, background_data)
         st = _lib.Settings(int(K), int(active_sh_bases), float(near_plane), float(far_plane), float(scale_modifier),
                            int(bool(to_chw)), int(bool(blur_periphery)), int(bool(aaa_mode)), bg_type,
-                           keep.f32(background_data, "background_data"), tw, th, int(bool(fast_math)))
+                           keep.f32(background_data, "background_data"), tw, th, int(bool(fast_math)),
+                           _lib.FOVEATION[foveation], float(rings[0]), float(rings[1]))
         sid = C.c_int32(-1)
         _lib.check(self._libh.fhtgs_server_add_scene(self.handle, C.byref(prims), C.byref(st), C.byref(sid)))
         with self._lock:

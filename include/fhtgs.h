@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FHTGS_ABI_VERSION 2
+#define FHTGS_ABI_VERSION 3
 
 typedef enum {
     FHTGS_OK = 0,
@@ -99,12 +99,34 @@ typedef struct {
     int32_t texture_width, texture_height;
     int32_t fast_math;         /* 1: arithmetic of _C_benchmarking/_C_stereo
                                   (-use_fast_math); 0: IEEE arithmetic of _C         */
+    int32_t foveation;         /* fhtgs_foveation; 0 = the reference's                */
+    float ring_full, ring_half;/* FHTGS_FOVEATION_RINGS: NDC radii (see below)        */
 } fhtgs_settings;
+
+/* Foveation modes (fhtgs_settings.foveation).
+ *   REFERENCE: the reference's fixed layout (config.h:30-35): 16x16 tiles whose centre lies
+ *     within 15 tiles (240 px) of the gaze tile at full resolution, up to 24 tiles (375 px)
+ *     at full resolution cross-faded into the periphery, the rest sampled at stride 2 and
+ *     upsampled bilinearly.  The only mode the reference has; the drop-in calls use it.
+ *   RINGS: no counterpart in the reference.  A tile whose centre lies at NDC distance
+ *     r < ring_full from the gaze (x and y each scaled by half the image size) is rendered at
+ *     full resolution, r < ring_half at stride 2, the rest at stride 4; strided tiles are
+ *     upsampled bilinearly from their own samples and the first row/column of their right and
+ *     lower neighbours (a 2x tile does not sample a 4x neighbour; masked neighbours are
+ *     clamped into the tile).  Ring boundaries are hard tile edges (no cross-fade).
+ *     blur_periphery is not available in this mode.
+ *   NONE: every visible tile at full resolution. */
+typedef enum {
+    FHTGS_FOVEATION_REFERENCE = 0,
+    FHTGS_FOVEATION_RINGS = 1,
+    FHTGS_FOVEATION_NONE = 2
+} fhtgs_foveation;
 
 /* Per-view facts of the last frame rendered by a context (read after it completed). */
 typedef struct {
     int64_t n_instances;       /* reference's M = sum of touched-tile counts (sub-tile copies
-                                  of fovea tiles and over-counted sentinel slots included) */
+                                  of fovea tiles and over-counted sentinel slots included);
+                                  in the RINGS / NONE foveation modes the stored count      */
     int64_t instance_capacity; /* stored-instance slots available per view                 */
     uint32_t n_active_tiles;   /* small-tile entries in the tile index map                 */
     uint32_t partition_ranges[6]; /* fovea, periphery, blended [begin,end)                 */
@@ -119,6 +141,8 @@ typedef struct {
  * tile appears once per sub-tile, and over-counted slots follow as sentinel keys (0xFFFF for
  * 16-bit keys, else 0xFFFFFFFF) with value 0xFFFFFFFF.  The renderer itself stores each list
  * once; these arrays are expanded from it exactly. */
+/* In the RINGS / NONE foveation modes there is no reference layout: keys, values and ranges
+ * hold each stored list once, keyed by its large tile's first sub-tile (4 * tile). */
 typedef struct {
     uint32_t* n_touched;      /* [N]           */
     uint16_t* screen_bounds;  /* [N,4]         */

@@ -850,6 +850,115 @@ void blend_compose(const oracle_view* v, const oracle_settings* st, const Geomet
     }
 }
 
+/* ---- ring / no foveation: no counterpart in the reference; restates the product's
+ *      FHTGS_FOVEATION_RINGS / _NONE modes (fhtgs_kernels.cuh: ring_tile_type, the blend's
+ *      stride-4 tiles, grid_sample4 and the stride-4 bilinear fill).  Per-tile lists are the
+ *      reference's (primitives in ascending order whose bounds hold the visible tile); each
+ *      tile is blended at stride 1, 2 or 4 with the reference's per-pixel arithmetic and
+ *      strided tiles are filled bilinearly. ---- */
+enum : uint8_t { LVL_FULL = 0, LVL_HALF = 1, LVL_MASKED = 3, LVL_QUARTER = 4 };
+
+uint8_t ring_level(const oracle_view* v, const oracle_settings* st, const Geometry& g, int tx, int ty) {
+    if (st->foveation == 2) return LVL_FULL;
+    const float cx = float(tx * kTileLarge + kTileLarge / 2), cy = float(ty * kTileLarge + kTileLarge / 2);
+    const float hx = 0.5f * float(v->width), hy = 0.5f * float(v->height);
+    const float dx = (cx - g.gaze_px) / hx, dy = (cy - g.gaze_py) / hy;
+    const float dxx = dx * dx, dyy = dy * dy;
+    const float r2 = dxx + dyy;
+    const float f2 = st->ring_full * st->ring_full, h2 = st->ring_half * st->ring_half;
+    return r2 < f2 ? LVL_FULL : r2 < h2 ? LVL_HALF : LVL_QUARTER;
+}
+
+/* (n x n) samples of the S-strided grid from (bx, by); a sample whose tile is masked, or
+ * (for the 2x grid) a 4x tile, is clamped into the large tile (ltx, lty). */
+void load_samples_rings(const ImageRef& src, const uint32_t* mask, const std::vector<uint8_t>& level, int glw,
+                        int bx, int by, int n, int S, int ltx, int lty, std::vector<V3<float>>& s) {
+    const int max_r = int((unsigned(src.W) - unsigned(bx) - 1u) / unsigned(S));
+    const int max_d = int((unsigned(src.H) - unsigned(by) - 1u) / unsigned(S));
+    s.resize(size_t(n) * n);
+    for (int sy = 0; sy < n; ++sy)
+        for (int sx = 0; sx < n; ++sx) {
+            int px = bx + std::min(sx, max_r) * S;
+            int py = by + std::min(sy, max_d) * S;
+            int tile = py / kTileLarge * glw + px / kTileLarge;
+            bool ok = (mask[tile / 32] & (1u << (tile % 32))) != 0 && !(S == kStride && level[tile] == LVL_QUARTER);
+            if (!ok) {
+                int cx = std::max(ltx * kTileLarge, std::min(ltx * kTileLarge + kTileLarge - S, px));
+                int cy = std::max(lty * kTileLarge, std::min(lty * kTileLarge + kTileLarge - S, py));
+                s[size_t(sy) * n + sx] = src.load(cx, cy);
+            } else {
+                s[size_t(sy) * n + sx] = src.load(px, py);
+            }
+        }
+}
+
+V3<float> bilinear_s(const std::vector<V3<float>>& s, int n, int S, int lx, int ly) {
+    int bx = lx / S, by = ly / S;
+    float xf = float(lx % S) / float(S), yf = float(ly % S) / float(S);
+    auto P = [&](int yy, int xx) { return s[size_t(yy) * n + xx]; };
+    V3<float> r = {0, 0, 0};
+    if (lx % S == 0) {
+        r = r + P(by, bx) * (1.0f - yf);
+        r = r + P(by + 1, bx) * yf;
+    } else if (ly % S == 0) {
+        r = r + P(by, bx) * (1.0f - xf);
+        r = r + P(by, bx + 1) * xf;
+    } else {
+        r = r + P(by, bx) * (1.0f - xf) * (1.0f - yf);
+        r = r + P(by, bx + 1) * xf * (1.0f - yf);
+        r = r + P(by + 1, bx) * (1.0f - xf) * yf;
+        r = r + P(by + 1, bx + 1) * xf * yf;
+    }
+    return r;
+}
+
+template <class T>
+void render_rings(const oracle_view* v, const oracle_settings* st, const Geometry& g, int n, const uint32_t* nt,
+                  const uint16_t* sb, const float* vpmt, const float* rgba, float* image) {
+    std::vector<std::vector<uint32_t>> lists(size_t(g.n_large));
+    for (int i = 0; i < n; ++i) {
+        if (nt[i] == 0) continue;
+        for (uint32_t ty = sb[4 * i + 2]; ty < sb[4 * i + 3]; ++ty)
+            for (uint32_t tx = sb[4 * i + 0]; tx < sb[4 * i + 1]; ++tx) {
+                const uint32_t t = ty * uint32_t(g.glw) + tx;
+                if (visible(v->visibility_mask, t)) lists[t].push_back(uint32_t(i));
+            }
+    }
+    std::vector<uint8_t> level(size_t(g.n_large), LVL_MASKED);
+    for (int t = 0; t < g.n_large; ++t)
+        if (visible(v->visibility_mask, t)) level[t] = ring_level(v, st, g, t % g.glw, t / g.glw);
+    ImageRef img{image, v->width, v->height, st->to_chw != 0};
+    #pragma omp parallel for schedule(dynamic, 4)
+    for (int t = 0; t < g.n_large; ++t) {
+        if (level[t] == LVL_MASKED) continue;
+        const int S = level[t] == LVL_FULL ? 1 : level[t] == LVL_HALF ? kStride : 4;
+        const int ox = (t % g.glw) * kTileLarge, oy = (t / g.glw) * kTileLarge;
+        const std::vector<uint32_t>& L = lists[t];
+        for (int y = 0; y < kTileLarge; y += S)
+            for (int x = 0; x < kTileLarge; x += S) {
+                if (ox + x >= v->width || oy + y >= v->height) continue;
+                blend_pixel<T>(v, st, vpmt, rgba, L.data(), 0, uint32_t(L.size()), ox + x, oy + y, img);
+            }
+    }
+    #pragma omp parallel for schedule(dynamic, 4)
+    for (int t = 0; t < g.n_large; ++t) {
+        if (level[t] != LVL_HALF && level[t] != LVL_QUARTER) continue;
+        const int S = level[t] == LVL_HALF ? kStride : 4;
+        const int ltx = t % g.glw, lty = t / g.glw, ox = ltx * kTileLarge, oy = lty * kTileLarge;
+        const int ns = kTileLarge / S + 1;
+        std::vector<V3<float>> smp;
+        load_samples_rings(img, v->visibility_mask, level, g.glw, ox, oy, ns, S, ltx, lty, smp);
+        for (int ly = 0; ly < kTileLarge; ++ly)
+            for (int lx = 0; lx < kTileLarge; ++lx) {
+                const int px = ox + lx, py = oy + ly;
+                if (px >= v->width || py >= v->height) continue;
+                if (lx % S == 0 && ly % S == 0) continue;
+                V3<float> r = bilinear_s(smp, ns, S, lx, ly);
+                img.store(px, py, sat_f(r.x), sat_f(r.y), sat_f(r.z));
+            }
+    }
+}
+
 struct ThreadScope {
     int prev = 0;
     explicit ThreadScope(int n) {
@@ -895,8 +1004,11 @@ int render_view_t(const oracle_scene* s, const oracle_view* v, const oracle_sett
     Inst I = instances(v, g, s->n, nt.data(), sb.data());
     if (image) {
         std::memset(image, 0, sizeof(float) * size_t(v->width) * v->height * 3);
-        blend_compose<T>(v, st, g, vpmt.data(), rgba.data(), tl.map_part.data(), tl.ranges, I.values.data(),
-                         I.ranges.data(), image);
+        if (st->foveation == 0)
+            blend_compose<T>(v, st, g, vpmt.data(), rgba.data(), tl.map_part.data(), tl.ranges, I.values.data(),
+                             I.ranges.data(), image);
+        else
+            render_rings<T>(v, st, g, s->n, nt.data(), sb.data(), vpmt.data(), rgba.data(), image);
     }
     if (prim) {
         if (prim->n_touched) std::memcpy(prim->n_touched, nt.data(), nt.size() * 4);

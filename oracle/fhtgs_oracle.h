@@ -56,6 +56,12 @@ typedef struct {
     int texture_width, texture_height;
     int precision;                   /* 32 or 64 */
     int n_threads;                   /* OpenMP threads, <=0: default            */
+    /* Foveation (as fhtgs_settings.foveation of the product): 0 the reference's; 1 rings
+     * (full resolution for NDC distance < ring_full from the gaze, stride 2 below ring_half,
+     * stride 4 beyond); 2 none (all tiles full resolution).  Modes 1 and 2 have no
+     * counterpart in the reference. */
+    int foveation;
+    float ring_full, ring_half;
 } oracle_settings;
 
 /* Per-primitive results of the preprocess stage (inference.cuh:42-136). */

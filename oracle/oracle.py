@@ -49,7 +49,10 @@ class OracleSettings(C.Structure):
         ("background_type", C.c_int), ("background_data", f32p),
         ("texture_width", C.c_int), ("texture_height", C.c_int),
         ("precision", C.c_int), ("n_threads", C.c_int),
+        ("foveation", C.c_int), ("ring_full", C.c_float), ("ring_half", C.c_float),
     ]
+
+FOVEATION = {"reference": 0, "rings": 1, "none": 2}
 
 
 class OraclePrimitives(C.Structure):
@@ -145,8 +148,11 @@ def make_scene(g, keep: _Keep) -> OracleScene:
 
 
 def make_settings(keep: _Keep, K=8, active_sh_bases=16, scale_modifier=1.0, to_chw=True, blur=False,
-                  aaa=False, background=None, background_type=0, precision=64, n_threads=0) -> OracleSettings:
+                  aaa=False, background=None, background_type=0, precision=64, n_threads=0,
+                  foveation="reference", rings=(0.15, 0.4)) -> OracleSettings:
     st = OracleSettings()
+    st.foveation = FOVEATION[foveation]
+    st.ring_full, st.ring_half = float(rings[0]), float(rings[1])
     st.K, st.active_sh_bases, st.scale_modifier = K, active_sh_bases, scale_modifier
     st.to_chw, st.blur_periphery, st.anti_aliasing = int(to_chw), int(blur), int(aaa)
     st.background_type = background_type
