@@ -1339,10 +1339,15 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
                 const float4 c = s_rgba[j];
                 const float alpha = fminf(c.w * G, kMaxFragmentAlpha);
                 if (alpha < kMinAlpha) continue;
-                const float3 ep = cross(d, m) * den_rcp;
-                const float depth = dot(xyz(VPMT4), ep) + VPMT4.w;
                 float4 pm = make_float4(c.x * alpha, c.y * alpha, c.z * alpha, alpha);
-                if (depth < core[K - 1].depth && alpha >= kMinAlphaCore) {
+                // the depth matters only to a fragment that may enter the core (alpha >= 1/20):
+                // evaluated under that test, so that warps whose fragments are all faint skip it
+                float depth = 3.402823466e+38f;
+                if (alpha >= kMinAlphaCore) {
+                    const float3 ep = cross(d, m) * den_rcp;
+                    depth = dot(xyz(VPMT4), ep) + VPMT4.w;
+                }
+                if (depth < core[K - 1].depth) {
                     Frag f;
                     f.depth = depth;
                     f.color = pack_rgba(pm);

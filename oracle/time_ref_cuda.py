@@ -7,6 +7,12 @@ blocking call, 10 warm-up calls, then --calls timed calls; median and p99 in ms,
 median.  Also checks that the two produce identical images on the workload.
 
     python oracle/time_ref_cuda.py [--calls 100] [--n 1000000] [--width 2064 --height 2208]
+    python oracle/time_ref_cuda.py --served [--duration 5 --rate 240]
+
+--served: the served-stream trace of bench.py --workload served (3 scenes of 0.5M/2M/4M SH3
+Gaussians, seeds 1-3, stereo requests of 1440x1584 or 2064x2208 per eye), every request issued
+back to back as one blocking `_C_stereo.render` call, through the reference and through this
+package's drop-in: requests/s of each (the plain per-request path at saturation).
 """
 from __future__ import annotations
 
@@ -39,6 +45,38 @@ def timed_calls(fn, calls: int, warmup: int = 10):
             "mean_ms": float(ms.mean()), "frames_per_s": float(1000.0 / np.median(ms)), "calls": calls}
 
 
+def served(a) -> dict:
+    import time
+
+    import torch
+
+    import foveatedhtgscudabackend_b200 as F
+    from foveatedhtgscudabackend_b200 import scene
+    import ref as REF
+
+    sizes = (500_000, 2_000_000, 4_000_000)
+    scenes = [F.gaussians_to_torch(scene.make_gaussians(n, 3, seed=i + 1)) for i, n in enumerate(sizes)]
+    trace = scene.make_served_requests(a.duration, a.rate, len(scenes), seed=0)
+    sts = [[F.settings_from_view(v, K=a.K, active_sh_bases=16) for v in (l, r)] for t, si, l, r in trace]
+    ref_mod = REF.module("_C_stereo")
+    out = {"workload": f"served trace: {len(trace)} stereo requests, scenes {sizes}, "
+                       f"1440x1584 or 2064x2208 per eye (bench.py --workload served, seed 0)"}
+    for name, mod in (("reference_cuda", ref_mod), ("ours_dropin", F._C_stereo)):
+        for k in range(6):  # warm-up
+            si = trace[k][1]
+            mod.render(*scenes[si], *sts[k][0].as_tuple(), *sts[k][1].as_tuple(), True, False, False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k, (t, si, l, r) in enumerate(trace):
+            mod.render(*scenes[si], *sts[k][0].as_tuple(), *sts[k][1].as_tuple(), True, False, False)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[name] = {"requests_per_s": len(trace) / dt, "seconds": dt}
+    out["speedup"] = out["ours_dropin"]["requests_per_s"] / out["reference_cuda"]["requests_per_s"]
+    out["gpu"] = torch.cuda.get_device_name()
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--calls", type=int, default=100)
@@ -46,7 +84,13 @@ def main(argv=None) -> int:
     ap.add_argument("--width", type=int, default=2064)
     ap.add_argument("--height", type=int, default=2208)
     ap.add_argument("--K", type=int, default=8)
+    ap.add_argument("--served", action="store_true")
+    ap.add_argument("--duration", type=float, default=5.0)
+    ap.add_argument("--rate", type=float, default=240.0)
     a = ap.parse_args(argv)
+    if a.served:
+        print(json.dumps(served(a)))
+        return 0
 
     import torch
 
