@@ -109,6 +109,7 @@ struct Layout {
     size_t off_views, off_status, off_nt, off_nvis, off_bounds, off_rec, off_bsums, off_keys0, off_keys1, off_vals0, off_vals1;
     size_t off_hist, off_dtot, off_ranges, off_map, off_type, off_ltype, off_wf, off_wl, off_wm, off_ctr, off_temp;
     size_t off_order0, off_order1;
+    size_t off_ghist, off_look, off_ticket;
     std::vector<size_t> temp_offsets;
 };
 
@@ -140,6 +141,9 @@ Layout plan(int V, int64_t N, int nbp, int64_t cap, int key_bytes, int sort_tile
     L.off_ctr = take(4ull * kCounterWords);
     L.off_order0 = take(4ull * V * max_large);
     L.off_order1 = take(4);
+    L.off_ghist = take(4ull * V * kSortMaxPasses * kSortBins);
+    L.off_look = take(4ull * V * kSortMaxPasses * sort_tiles * kSortBins);
+    L.off_ticket = take(4ull * V * kSortMaxPasses);
     for (int64_t f : temp_floats) L.temp_offsets.push_back(f > 0 ? take(4ull * f) : 0);
     L.total = o;
     return L;
@@ -319,6 +323,11 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     fb.counters = reinterpret_cast<uint32_t*>(A + L.off_ctr);
     fb.work_order[0] = reinterpret_cast<uint32_t*>(A + L.off_order0);
     fb.work_order[1] = reinterpret_cast<uint32_t*>(A + L.off_order1);
+    if (cap < kOnesweepMaxCap) {  // onesweep sort (look-back counts are 30-bit)
+        fb.sort_ghist = reinterpret_cast<uint32_t*>(A + L.off_ghist);
+        fb.sort_look = reinterpret_cast<uint32_t*>(A + L.off_look);
+        fb.sort_ticket = reinterpret_cast<uint32_t*>(A + L.off_ticket);
+    }
 
     std::vector<ViewSetup> setups(V);
     for (int i = 0; i < V; ++i) {
@@ -420,6 +429,8 @@ fhtgs_status render_sync_impl(fhtgs_context ctx, const fhtgs_primitives* prims, 
         for (int i = 0; i < n_views; ++i) {
             need = std::max(need, ctx->h_status[i].n_instances);
             overflow = overflow || ctx->h_status[i].n_instances > static_cast<unsigned long long>(ctx->cap);
+            if (ctx->h_status[i].overflow & kFrameErrSortLookback)
+                return fail(FHTGS_ERR_CUDA, "instance sort: a look-back wait gave up (view " + std::to_string(i) + ")");
         }
         if (!overflow) return FHTGS_OK;
         int64_t grown = static_cast<int64_t>(need + need / 4 + kSortTile);

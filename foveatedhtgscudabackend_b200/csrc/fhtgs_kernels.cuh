@@ -518,7 +518,7 @@ __device__ __forceinline__ bool transform_and_cull_aaa(const ViewParams& vp, con
 
 // AttrT: element type of scales/rotations/opacities; ShT: of sh_0/sh_rest.
 template <typename AttrT, typename ShT>
-__global__ void __launch_bounds__(kPrimBlock) preprocess_kernel(FrameParams fp, FrameBuffers fb, Gaussians g) {
+__global__ void __launch_bounds__(kPrimBlock, 3) preprocess_kernel(FrameParams fp, FrameBuffers fb, Gaussians g) {
     __shared__ uint32_t s_warp[33];
     const int i = blockIdx.x * kPrimBlock + threadIdx.x;
     const bool valid = i < fp.n_prims;
@@ -602,6 +602,11 @@ __global__ void __launch_bounds__(1024) scan_blocks_kernel(FrameParams fp, Frame
         fb.status[v].n_instances = static_cast<uint32_t>(carry);
         fb.status[v].overflow = static_cast<uint32_t>(carry) > static_cast<unsigned long long>(fp.cap) ? 1u : 0u;
     }
+    if (fb.sort_ghist) {  // onesweep sort: digit counts (filled by create) and tile tickets start at 0
+        for (int k = threadIdx.x; k < kSortMaxPasses * kSortBins; k += blockDim.x)
+            fb.sort_ghist[static_cast<size_t>(v) * kSortMaxPasses * kSortBins + k] = 0u;
+        if (threadIdx.x < kSortMaxPasses) fb.sort_ticket[v * kSortMaxPasses + threadIdx.x] = 0u;
+    }
 }
 
 int launch_scan_blocks(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s) {
@@ -620,9 +625,27 @@ constexpr uint32_t kSeqTiles = 16;   // bounds tiles handled by the owning threa
 constexpr uint32_t kNoPrimitive = 0xFFFFFFFFu;  // value of a sentinel instance slot
 constexpr int kBigList = kPrimBlock;
 
+// Stored instances the sort and the later stages see: the count, capped at the capacity.
+__device__ __forceinline__ uint64_t view_count(const FrameParams& fp, const FrameBuffers& fb, int v) {
+    const unsigned long long m = fb.status[v].n_instances;
+    return m < static_cast<unsigned long long>(fp.cap) ? m : static_cast<unsigned long long>(fp.cap);
+}
+
+__host__ __device__ __forceinline__ int sort_passes(const FrameParams& fp) {
+    return (fp.end_bit + kSortRadixBits - 1) / kSortRadixBits;
+}
+
+// Onesweep sort support in the creation kernel: every key written is counted into the block's
+// digit histogram of each pass (added to fb.sort_ghist at the end), and the view's look-back
+// words of the tiles the sort will use are cleared (the sort runs after this kernel).
+__device__ __forceinline__ void count_key(uint32_t* s_hist, int passes, uint32_t key) {
+    for (int p = 0; p < passes; ++p) atomicAdd(&s_hist[p * kSortBins + ((key >> (p * kSortRadixBits)) & (kSortBins - 1))], 1u);
+}
+
 template <typename KeyT>
 __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParams fp, FrameBuffers fb) {
     __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_dhist[kSortMaxPasses * kSortBins];
     __shared__ uint32_t s_big_n;
     __shared__ uint32_t s_big_prim[kBigList];
     __shared__ uint32_t s_big_off[kBigList];
@@ -640,7 +663,23 @@ __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParam
     KeyT* keys = reinterpret_cast<KeyT*>(fb.keys[0]) + static_cast<size_t>(v) * fp.cap;
     uint32_t* vals = fb.vals[0] + static_cast<size_t>(v) * fp.cap;
     const uint32_t glw = static_cast<uint32_t>(vp.glw);
+    const bool onesweep = fb.sort_ghist != nullptr;
+    const int passes = sort_passes(fp);
     if (threadIdx.x == 0) s_big_n = 0;
+    if (onesweep) {
+        for (int k = threadIdx.x; k < kSortMaxPasses * kSortBins; k += kPrimBlock) s_dhist[k] = 0u;
+        // look-back words of this view's tiles: [pass][tile][digit], tiles of the stored count
+        const uint64_t m = view_count(fp, fb, v);
+        const uint64_t tile = static_cast<uint64_t>(kSortThreads) * fb.sort_items;
+        const uint64_t per_pass = ((m + tile - 1) / tile) * kSortBins;
+        const uint64_t pass_stride = static_cast<uint64_t>(fb.sort_tiles) * kSortBins;
+        uint32_t* look = fb.sort_look + static_cast<size_t>(v) * kSortMaxPasses * pass_stride;
+        for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * kPrimBlock + threadIdx.x; k < passes * per_pass;
+             k += static_cast<uint64_t>(gridDim.x) * kPrimBlock) {
+            const uint64_t p = k / per_pass;
+            look[p * pass_stride + (k - p * per_pass)] = 0u;
+        }
+    }
     __syncthreads();
     if (nv > 0) {
         const ushort4 b = fb.bounds[o];
@@ -655,6 +694,7 @@ __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParam
                 if (w < lim) {
                     keys[w] = static_cast<KeyT>(tile);
                     vals[w] = static_cast<uint32_t>(i);
+                    if (onesweep) count_key(s_dhist, passes, tile);
                 }
                 ++w;
             }
@@ -663,6 +703,7 @@ __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParam
             for (; w < end && w < lim; ++w) {
                 keys[w] = static_cast<KeyT>(~KeyT(0));
                 vals[w] = kNoPrimitive;
+                if (onesweep) count_key(s_dhist, passes, static_cast<KeyT>(~KeyT(0)));
             }
         } else {
             const uint32_t slot = atomicAdd(&s_big_n, 1u);
@@ -695,13 +736,21 @@ __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParam
             if (c && w < lim && w < end) {
                 keys[w] = static_cast<KeyT>(tile);
                 vals[w] = prim;
+                if (onesweep) count_key(s_dhist, passes, tile);
             }
             w0 += step;
         }
         for (uint64_t w = w0 + threadIdx.x; w < end && w < lim; w += kPrimBlock) {  // see above
             keys[w] = static_cast<KeyT>(~KeyT(0));
             vals[w] = kNoPrimitive;
+            if (onesweep) count_key(s_dhist, passes, static_cast<KeyT>(~KeyT(0)));
         }
+    }
+    if (onesweep) {
+        __syncthreads();
+        uint32_t* gh = fb.sort_ghist + static_cast<size_t>(v) * kSortMaxPasses * kSortBins;
+        for (int k = threadIdx.x; k < passes * kSortBins; k += kPrimBlock)
+            if (s_dhist[k]) atomicAdd(&gh[k], s_dhist[k]);
     }
 }
 
@@ -719,10 +768,6 @@ int launch_create(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s)
 // __match_any_sync per warp; counts per (digit, tile) scanned digit-major; the scatter goes
 // through shared memory so that global stores run along digit runs.
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ uint64_t view_count(const FrameParams& fp, const FrameBuffers& fb, int v) {
-    const unsigned long long m = fb.status[v].n_instances;
-    return m < static_cast<unsigned long long>(fp.cap) ? m : static_cast<unsigned long long>(fp.cap);
-}
 
 template <typename KeyT, int ITEMS>
 __global__ void __launch_bounds__(kSortThreads) sort_upsweep_kernel(FrameParams fp, FrameBuffers fb, int buf, int shift) {
@@ -857,9 +902,160 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_scatter_kernel(FramePara
     }
 }
 
+// Onesweep pass (one kernel per 8-bit digit, after Adinets & Merrill, "Onesweep: a faster
+// least significant digit radix sort for GPUs", 2022): a block takes the next tile of the view
+// from a ticket counter (so every earlier tile belongs to a block that already runs), ranks
+// its keys once per key with __match_any_sync (stable: warps own consecutive key runs, visited
+// in key order), publishes its digit counts, and finds the counts of all earlier tiles by
+// decoupled look-back over their published words: flag kLookAggregate = this tile's own
+// count, kLookPrefix = the inclusive count of every tile up to it.  The digit's global start
+// is the exclusive sum of the pass's digit histogram (filled by the creation kernel).  The
+// look-back wait is bounded: a word that stays unpublished for kLookSpinLimit reads sets
+// kFrameErrSortLookback in the frame status and the pass goes on (the host reports the error).
+constexpr uint32_t kLookAggregate = 1u, kLookPrefix = 2u;
+constexpr uint32_t kLookCountMask = (1u << 30) - 1u;
+constexpr int kLookSpinLimit = 1 << 22;
+
+__device__ __forceinline__ uint32_t ld_look(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_look(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <typename KeyT, int ITEMS>
+__global__ void __launch_bounds__(kSortThreads, 3) sort_onesweep_kernel(FrameParams fp, FrameBuffers fb, int buf, int pass) {
+    constexpr int TILE = kSortThreads * ITEMS;
+    __shared__ uint32_t s_whist[kSortThreads / 32][kSortBins];  // per-warp counts, then warp starts
+    __shared__ uint32_t s_local_start[kSortBins];
+    __shared__ uint32_t s_global_start[kSortBins];
+    __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_tile, s_err;
+    __shared__ KeyT s_keys[TILE];
+    __shared__ uint32_t s_vals[TILE];
+    const int v = blockIdx.y;
+    const int shift = pass * kSortRadixBits;
+    const uint64_t M = view_count(fp, fb, v);
+    if (threadIdx.x == 0) {
+        s_tile = atomicAdd(&fb.sort_ticket[v * kSortMaxPasses + pass], 1u);
+        s_err = 0u;
+    }
+    for (int k = threadIdx.x; k < (kSortThreads / 32) * kSortBins; k += kSortThreads) (&s_whist[0][0])[k] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint64_t t0 = static_cast<uint64_t>(tile) * TILE;
+    if (t0 >= M) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lanemask_lt = (1u << lane) - 1u;
+    const uint32_t n_here = static_cast<uint32_t>(M - t0 < static_cast<uint64_t>(TILE) ? M - t0 : TILE);
+    const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[buf]) + static_cast<size_t>(v) * fp.cap + t0;
+    const uint32_t* vals = fb.vals[buf] + static_cast<size_t>(v) * fp.cap + t0;
+    KeyT* okeys = reinterpret_cast<KeyT*>(fb.keys[buf ^ 1]) + static_cast<size_t>(v) * fp.cap;
+    uint32_t* ovals = fb.vals[buf ^ 1] + static_cast<size_t>(v) * fp.cap;
+    const uint32_t wbase = static_cast<uint32_t>(warp) * 32 * ITEMS + lane;
+    KeyT k_reg[ITEMS];
+    uint32_t v_reg[ITEMS];
+    uint32_t rank[ITEMS];  // same-digit keys of this warp before the key
+#pragma unroll
+    for (int it = 0; it < ITEMS; ++it) {
+        const uint32_t idx = wbase + it * 32;
+        const bool ok = idx < n_here;
+        k_reg[it] = ok ? keys[idx] : static_cast<KeyT>(0);
+        v_reg[it] = ok ? vals[idx] : 0u;
+    }
+#pragma unroll
+    for (int it = 0; it < ITEMS; ++it) {
+        const bool ok = wbase + it * 32 < n_here;
+        const uint32_t d = ok ? (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1) : kSortBins;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t base = ok ? s_whist[warp][d] : 0u;
+        __syncwarp();
+        rank[it] = base + __popc(peers & lanemask_lt);
+        if (ok && lane == __ffs(peers) - 1) s_whist[warp][d] = base + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // digit d (thread d): warp starts and the tile's count
+    const int d = threadIdx.x;
+    uint32_t cnt = 0, wpre[kSortThreads / 32];
+#pragma unroll
+    for (int w = 0; w < kSortThreads / 32; ++w) {
+        wpre[w] = cnt;
+        cnt += s_whist[w][d];
+    }
+    uint32_t tile_total;
+    const uint32_t lstart = block_excl_scan<uint32_t>(cnt, tile_total, s_warp);
+    // publish this tile's count, then look back over the earlier tiles for this digit
+    uint32_t* look = fb.sort_look + (static_cast<size_t>(v) * kSortMaxPasses + pass) * fb.sort_tiles * kSortBins;
+    st_look(look + static_cast<size_t>(tile) * kSortBins + d, ((tile == 0 ? kLookPrefix : kLookAggregate) << 30) | cnt);
+    uint32_t excl = 0;
+    if (tile > 0) {
+        int64_t t = static_cast<int64_t>(tile) - 1;
+        int spins = 0;
+        while (t >= 0) {
+            const uint32_t w = ld_look(look + static_cast<size_t>(t) * kSortBins + d);
+            const uint32_t flag = w >> 30;
+            if (flag == 0u) {
+                if (++spins > kLookSpinLimit) {
+                    atomicOr(&fb.status[v].overflow, kFrameErrSortLookback);
+                    s_err = 1u;
+                    break;
+                }
+                __nanosleep(32);
+                continue;
+            }
+            excl += w & kLookCountMask;
+            if (flag == kLookPrefix) break;
+            --t;
+        }
+        st_look(look + static_cast<size_t>(tile) * kSortBins + d, (kLookPrefix << 30) | ((excl + cnt) & kLookCountMask));
+    }
+    uint32_t all_total;
+    const uint32_t dbase = block_excl_scan<uint32_t>(
+        fb.sort_ghist[(static_cast<size_t>(v) * kSortMaxPasses + pass) * kSortBins + d], all_total, s_warp);
+    s_local_start[d] = lstart;
+    s_global_start[d] = dbase + excl;
+#pragma unroll
+    for (int w = 0; w < kSortThreads / 32; ++w) s_whist[w][d] = lstart + wpre[w];  // first slot of warp w
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < ITEMS; ++it) {
+        if (wbase + it * 32 < n_here) {
+            const uint32_t dd = (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1);
+            const uint32_t p = s_whist[warp][dd] + rank[it];
+            s_keys[p] = k_reg[it];
+            s_vals[p] = v_reg[it];
+        }
+    }
+    __syncthreads();
+    if (s_err) return;  // a look-back gave up: no position of this tile can be trusted
+    for (uint32_t j = threadIdx.x; j < n_here; j += kSortThreads) {
+        const KeyT kk = s_keys[j];
+        const uint32_t dd = (static_cast<uint32_t>(kk) >> shift) & (kSortBins - 1);
+        const uint32_t gpos = s_global_start[dd] + (j - s_local_start[dd]);
+        if (gpos < M) {
+            okeys[gpos] = kk;
+            ovals[gpos] = s_vals[j];
+        }
+    }
+}
+
 // fb.sort_tiles must be ceil(cap / (kSortThreads * ITEMS)).
 template <typename KeyT, int ITEMS>
 int sort_t(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s) {
+    if (fb.sort_look) {  // onesweep: one kernel per pass
+        const int passes = sort_passes(fp);
+        dim3 gt(fb.sort_tiles, fp.n_views);
+        int buf = 0;
+        for (int p = 0; p < passes; ++p) {
+            sort_onesweep_kernel<KeyT, ITEMS><<<gt, kSortThreads, 0, s>>>(fp, fb, buf, p);
+            buf ^= 1;
+        }
+        fb.final_buf = buf;
+        return passes;
+    }
     const int passes = (fp.end_bit + kSortRadixBits - 1) / kSortRadixBits;
     int buf = 0;
     dim3 gt(fb.sort_tiles, fp.n_views), gd(kSortBins, fp.n_views);

@@ -142,6 +142,10 @@ struct FrameBuffers {
     uint32_t* work_masked;    // [V][max_large] masked large tiles
     uint32_t* counters;       // [kCounterWords]: work counters, then the work-order buckets
     uint32_t* work_order[2];  // [0]: [V*max_large] packed blend items, heaviest first; [1] unused
+    // Onesweep sort state (null: the three-kernel sort, which needs sort_hist/sort_digit_tot):
+    uint32_t* sort_ghist;     // [V][kSortMaxPasses][256] digit counts of every pass (create fills)
+    uint32_t* sort_look;      // [V][kSortMaxPasses][sort_tiles][256] look-back words
+    uint32_t* sort_ticket;    // [V][kSortMaxPasses] tiles handed out so far
 };
 
 // Work ordering: tiles are bucketed by list length in quarter octaves and blended in
@@ -178,5 +182,10 @@ constexpr int kSortItemsMin = 8;      // smallest tile the autotuner may choose 
 constexpr int kBlendRowChoices[3] = {8, 16, 4};
 constexpr int kSortRadixBits = 8;
 constexpr int kSortBins = 1 << kSortRadixBits;
+constexpr int kSortMaxPasses = 3;     // keys of at most 24 significant bits (tile ids < 2^24)
+// Look-back words of the onesweep sort: 2 flag bits over a 30-bit count, so the onesweep path
+// needs an instance capacity below 2^30 per view (larger arenas use the three-kernel sort).
+constexpr int64_t kOnesweepMaxCap = int64_t(1) << 30;
+constexpr uint32_t kFrameErrSortLookback = 2u;  // FrameStatus.overflow bit: look-back gave up
 
 }  // namespace fhtgs
