@@ -431,6 +431,8 @@ fhtgs_status render_sync_impl(fhtgs_context ctx, const fhtgs_primitives* prims, 
             overflow = overflow || ctx->h_status[i].n_instances > static_cast<unsigned long long>(ctx->cap);
             if (ctx->h_status[i].overflow & kFrameErrSortLookback)
                 return fail(FHTGS_ERR_CUDA, "instance sort: a look-back wait gave up (view " + std::to_string(i) + ")");
+            if (ctx->h_status[i].overflow & kFrameErrStaging)
+                return fail(FHTGS_ERR_CUDA, "preprocess: attribute staging did not complete (view " + std::to_string(i) + ")");
         }
         if (!overflow) return FHTGS_OK;
         int64_t grown = static_cast<int64_t>(need + need / 4 + kSortTile);

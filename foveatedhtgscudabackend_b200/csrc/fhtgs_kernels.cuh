@@ -516,26 +516,116 @@ __device__ __forceinline__ bool transform_and_cull_aaa(const ViewParams& vp, con
     return n == 0;
 }
 
-// AttrT: element type of scales/rotations/opacities; ShT: of sh_0/sh_rest.
+// ---- bulk-copy (TMA) staging of a block's Gaussian attributes into shared memory ----------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// One contiguous global -> shared copy by the bulk-copy engine, completing on `bar` (no
+// multicast: this CTA's own shared memory).  dst, src and bytes are multiples of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// Bounded wait for the staging barrier: true when the copies landed.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int limit) {
+    for (int k = 0; k < limit; ++k)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+constexpr int kStageWaitLimit = 1 << 20;
+
+// Bytes of one block's staged attributes (kPrimBlock Gaussians, each array 16-byte padded).
 template <typename AttrT, typename ShT>
+__host__ __device__ __forceinline__ uint32_t staged_bytes(int total_sh) {
+    return kPrimBlock * (12u + 3u * sizeof(AttrT) + 4u * sizeof(AttrT) + sizeof(AttrT) + 3u * sizeof(ShT) +
+                         3u * static_cast<uint32_t>(total_sh) * sizeof(ShT));
+}
+constexpr uint32_t kMaxStagedBytes = 72 * 1024;  // 3 blocks per SM
+
+// AttrT: element type of scales/rotations/opacities; ShT: of sh_0/sh_rest.
+// `staged`: full blocks copy their attributes into shared memory with the bulk-copy engine
+// (the arrays are contiguous per block: kPrimBlock x {12, 3, 4, 1, 3, 3S} elements) and every
+// thread then reads its Gaussian from there; the last partial block, and launches whose arrays
+// are not 16-byte aligned, read global memory directly.  Same values either way.
+template <typename AttrT, typename ShT, bool STAGED>
 __global__ void __launch_bounds__(kPrimBlock, 3) preprocess_kernel(FrameParams fp, FrameBuffers fb, Gaussians g) {
+    extern __shared__ __align__(128) unsigned char s_stage[];
     __shared__ uint32_t s_warp[33];
-    const int i = blockIdx.x * kPrimBlock + threadIdx.x;
+    __shared__ uint64_t s_bar;
+    const int i0 = blockIdx.x * kPrimBlock;
+    const int i = i0 + threadIdx.x;
     const bool valid = i < fp.n_prims;
     const int ii = valid ? i : 0;
+    const float* positions = g.positions;
     const AttrT* scales = reinterpret_cast<const AttrT*>(g.scales);
     const AttrT* rotations = reinterpret_cast<const AttrT*>(g.rotations);
     const AttrT* opacities = reinterpret_cast<const AttrT*>(g.opacities);
     const ShT* sh_0 = reinterpret_cast<const ShT*>(g.sh_0);
     const ShT* sh_rest = reinterpret_cast<const ShT*>(g.sh_rest);
+    size_t li = static_cast<size_t>(ii);  // index into the arrays read below
+    if (STAGED && i0 + kPrimBlock <= fp.n_prims) {
+        const uint32_t S3 = 3u * static_cast<uint32_t>(fp.total_sh);
+        const uint32_t b_pos = kPrimBlock * 12u, b_sc = kPrimBlock * 3u * sizeof(AttrT),
+                       b_rot = kPrimBlock * 4u * sizeof(AttrT), b_op = kPrimBlock * sizeof(AttrT),
+                       b_sh0 = kPrimBlock * 3u * sizeof(ShT), b_shr = kPrimBlock * S3 * sizeof(ShT);
+        unsigned char* d_pos = s_stage;
+        unsigned char* d_sc = d_pos + b_pos;
+        unsigned char* d_rot = d_sc + b_sc;
+        unsigned char* d_op = d_rot + b_rot;
+        unsigned char* d_sh0 = d_op + b_op;
+        unsigned char* d_shr = d_sh0 + b_sh0;
+        if (threadIdx.x == 0) mbar_init(&s_bar, 1u);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            mbar_arrive_expect_tx(&s_bar, b_pos + b_sc + b_rot + b_op + b_sh0 + b_shr);
+            bulk_g2s(d_pos, positions + 3 * static_cast<size_t>(i0), b_pos, &s_bar);
+            bulk_g2s(d_sc, scales + 3 * static_cast<size_t>(i0), b_sc, &s_bar);
+            bulk_g2s(d_rot, rotations + 4 * static_cast<size_t>(i0), b_rot, &s_bar);
+            bulk_g2s(d_op, opacities + static_cast<size_t>(i0), b_op, &s_bar);
+            bulk_g2s(d_sh0, sh_0 + 3 * static_cast<size_t>(i0), b_sh0, &s_bar);
+            if (b_shr) bulk_g2s(d_shr, sh_rest + static_cast<size_t>(S3) * i0, b_shr, &s_bar);
+        }
+        const bool late = __syncthreads_or(!mbar_wait_bounded(&s_bar, 0u, kStageWaitLimit));
+        if (late) {
+            // flag the frame, give the copies a second bounded wait, and leave this block's
+            // Gaussians unwritten (the host reports the frame as failed)
+            if (threadIdx.x == 0) for (int v = 0; v < fp.n_views; ++v) atomicOr(&fb.status[v].overflow, kFrameErrStaging);
+            __syncthreads_or(!mbar_wait_bounded(&s_bar, 0u, kStageWaitLimit));
+            return;
+        }
+        positions = reinterpret_cast<const float*>(d_pos);
+        scales = reinterpret_cast<const AttrT*>(d_sc);
+        rotations = reinterpret_cast<const AttrT*>(d_rot);
+        opacities = reinterpret_cast<const AttrT*>(d_op);
+        sh_0 = reinterpret_cast<const ShT*>(d_sh0);
+        sh_rest = reinterpret_cast<const ShT*>(d_shr);
+        li = threadIdx.x;
+    }
     float3 pos = make_float3(0.f, 0.f, 0.f), scale = pos;
     float4 quat = make_float4(1.f, 0.f, 0.f, 0.f);
     float op = 0.0f;
     if (valid) {
-        pos = ld3(g.positions + 3 * static_cast<size_t>(ii));
-        scale = ld3t(scales + 3 * static_cast<size_t>(ii));
-        quat = ld4t(rotations + 4 * static_cast<size_t>(ii));
-        op = ldf(opacities + ii);
+        pos = ld3(positions + 3 * li);
+        scale = ld3t(scales + 3 * li);
+        quat = ld4t(rotations + 4 * li);
+        op = ldf(opacities + li);
     }
     const size_t N = static_cast<size_t>(fp.n_prims);
     for (int v = 0; v < fp.n_views; ++v) {
@@ -554,9 +644,8 @@ __global__ void __launch_bounds__(kPrimBlock, 3) preprocess_kernel(FrameParams f
             if (!culled) {
                 fb.bounds[o] = make_ushort4(static_cast<unsigned short>(b.x), static_cast<unsigned short>(b.y),
                                             static_cast<unsigned short>(b.z), static_cast<unsigned short>(b.w));
-                const float3 rgb = sh_to_rgb(sh_0 + 3 * static_cast<size_t>(ii),
-                                             sh_rest + static_cast<size_t>(3) * fp.total_sh * ii, pos, xyz(vp.cam),
-                                             fp.active_sh);
+                const float3 rgb = sh_to_rgb(sh_0 + 3 * li, sh_rest + static_cast<size_t>(3) * fp.total_sh * li, pos,
+                                             xyz(vp.cam), fp.active_sh);
                 float4* r = fb.rec + 4 * o;
                 r[0] = P1;
                 r[1] = P2;
@@ -574,10 +663,32 @@ __global__ void __launch_bounds__(kPrimBlock, 3) preprocess_kernel(FrameParams f
     }
 }
 
+// Staging is used by the fast-math flavour only: the IEEE flavour (the reference's _C) keeps
+// direct loads, whose compiled arithmetic is the one pinned bit for bit against the reference.
+template <typename AttrT, typename ShT>
+void launch_preprocess_t(const FrameParams& fp, const FrameBuffers& fb, const Gaussians& g, cudaStream_t s) {
+    const uint32_t bytes = staged_bytes<AttrT, ShT>(fp.total_sh);
+    auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    const bool staged = kStagedPreprocess && bytes <= kMaxStagedBytes && aligned(g.positions) && aligned(g.scales) &&
+                        aligned(g.rotations) && aligned(g.opacities) && aligned(g.sh_0) &&
+                        (fp.total_sh == 0 || aligned(g.sh_rest));
+    if (!staged) {
+        preprocess_kernel<AttrT, ShT, false><<<fp.n_blocks_prim, kPrimBlock, 0, s>>>(fp, fb, g);
+        return;
+    }
+    static bool configured = false;  // per instantiation: allow the staging buffer's size
+    if (!configured) {
+        cudaFuncSetAttribute(preprocess_kernel<AttrT, ShT, kStagedPreprocess>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kMaxStagedBytes));
+        configured = true;
+    }
+    preprocess_kernel<AttrT, ShT, kStagedPreprocess><<<fp.n_blocks_prim, kPrimBlock, bytes, s>>>(fp, fb, g);
+}
+
 int launch_preprocess(const FrameParams& fp, const FrameBuffers& fb, const Gaussians& g, cudaStream_t s) {
     if (fp.n_blocks_prim == 0) return 0;
-    if (g.half) preprocess_kernel<__half, __nv_bfloat16><<<fp.n_blocks_prim, kPrimBlock, 0, s>>>(fp, fb, g);
-    else preprocess_kernel<float, float><<<fp.n_blocks_prim, kPrimBlock, 0, s>>>(fp, fb, g);
+    if (g.half) launch_preprocess_t<__half, __nv_bfloat16>(fp, fb, g, s);
+    else launch_preprocess_t<float, float>(fp, fb, g, s);
     return 1;
 }
 

@@ -187,5 +187,6 @@ constexpr int kSortMaxPasses = 3;     // keys of at most 24 significant bits (ti
 // needs an instance capacity below 2^30 per view (larger arenas use the three-kernel sort).
 constexpr int64_t kOnesweepMaxCap = int64_t(1) << 30;
 constexpr uint32_t kFrameErrSortLookback = 2u;  // FrameStatus.overflow bit: look-back gave up
+constexpr uint32_t kFrameErrStaging = 4u;   // FrameStatus.overflow bit: attribute staging timed out
 
 }  // namespace fhtgs
