@@ -1640,17 +1640,21 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
                 const float3 d = cross(nx, ny);
                 const float num = dot(m, m);
                 const float den = dot(d, d);
-                if (num > kMaxCutoffSq * den) continue;
+                // In almost every warp step some lane passes both tests, so the fragment is
+                // evaluated for every lane and the tests only gate its effects (no divergent
+                // exits; a lane that failed cannot contribute: its `frag` is false whatever
+                // rcp/exp return for it).
+                const bool live = !(num > kMaxCutoffSq * den);
                 const float den_rcp = 1.0f / den;
                 const float G = expf(-0.5f * num * den_rcp);
                 const float4 c = s_rgba[j];
                 const float alpha = fminf(c.w * G, kMaxFragmentAlpha);
-                if (alpha < kMinAlpha) continue;
+                const bool frag = live && !(alpha < kMinAlpha);
                 float4 pm = make_float4(c.x * alpha, c.y * alpha, c.z * alpha, alpha);
                 // the depth matters only to a fragment that may enter the core (alpha >= 1/20):
                 // evaluated under that test, so that warps whose fragments are all faint skip it
                 float depth = 3.402823466e+38f;
-                if (alpha >= kMinAlphaCore) {
+                if (frag && alpha >= kMinAlphaCore) {
                     const float3 ep = cross(d, m) * den_rcp;
                     depth = dot(xyz(VPMT4), ep) + VPMT4.w;
                 }
@@ -1668,9 +1672,11 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
                     }
                     pm = unpack_rgba(f.color);
                 }
-                const float pt = 1.0f - pm.w;
-                tail += pm;
-                tail_T *= pt;
+                if (frag) {
+                    const float pt = 1.0f - pm.w;
+                    tail += pm;
+                    tail_T *= pt;
+                }
             }
         }
         if (inside) {
