@@ -1249,7 +1249,7 @@ __device__ __forceinline__ int items_of_view(const FrameStatus& st) {
 }
 
 __device__ __forceinline__ int cost_bucket(uint32_t cost) {
-    return cost == 0 ? 0 : min(kOrderBuckets - 1, 1 + __float2int_rd(4.0f * __log2f(static_cast<float>(cost))));
+    return cost == 0 ? 0 : min(kCostBuckets - 1, 1 + __float2int_rd(4.0f * __log2f(static_cast<float>(cost))));
 }
 
 // Maps flat item g to (view, index within the view); `pre` holds the exclusive prefix of the
@@ -1280,6 +1280,18 @@ __device__ __forceinline__ uint32_t item_cost(const FrameParams& fp, const Frame
     return len * (quarter ? 1u : low ? 2u : 8u);
 }
 
+// Work-list bucket of an item: its class (full resolution 2, periphery 1, quarter 0) above its
+// cost bucket, so that the descending scatter lists every full-resolution tile first (all 8
+// warps of a block busy), then the periphery tiles, then the quarter tiles, each class heaviest
+// first; a strided tile then never holds a block that full-resolution work is waiting for.
+__device__ __forceinline__ int item_bucket(const FrameParams& fp, const FrameBuffers& fb, int v, int j, uint32_t& packed) {
+    const uint32_t cost = item_cost(fp, fb, v, j, packed);
+    const FrameStatus& st = fb.status[v];
+    const int n_full = static_cast<int>(st.n_fovea_large + st.n_blended_large);
+    const int cls = j < n_full ? 2 : (j - n_full) < static_cast<int>(st.n_periphery_large) ? 1 : 0;
+    return cls * kCostBuckets + cost_bucket(cost);
+}
+
 constexpr int kMaxOrderViews = 1024;
 
 // Per-view prefix of the item counts into shared memory; returns the total.
@@ -1307,7 +1319,7 @@ __global__ void __launch_bounds__(256) order_hist_kernel(FrameParams fp, FrameBu
         int v, j;
         item_of(g, pre, fp.n_views, v, j);
         uint32_t packed;
-        atomicAdd(&hist[cost_bucket(item_cost(fp, fb, v, j, packed))], 1u);
+        atomicAdd(&hist[item_bucket(fp, fb, v, j, packed)], 1u);
     }
     __syncthreads();
     uint32_t* gh = fb.counters + 4;
@@ -1334,7 +1346,7 @@ __global__ void __launch_bounds__(256) order_scatter_kernel(FrameParams fp, Fram
         int v, j;
         item_of(g, pre, fp.n_views, v, j);
         uint32_t packed;
-        const int b = cost_bucket(item_cost(fp, fb, v, j, packed));
+        const int b = item_bucket(fp, fb, v, j, packed);
         out[base[b] + atomicAdd(&cursor[b], 1u)] = packed;
     }
 }
@@ -1517,14 +1529,189 @@ __device__ __forceinline__ bool conic_meets_rect(const Conic& q, float ax0, floa
 // dominates for large K.
 __host__ __device__ constexpr int blend_min_blocks(int K) { return K >= 32 ? 2 : K >= 16 ? 3 : 4; }
 
-// One persistent kernel blends every tile of every view.  A block takes the next item of the
-// ordered work list and renders one 16x16 area: a full-resolution tile with its 8 warps (each
-// RW x 32/RW pixels: 8 x 4 laid out 2 x 4, 16 x 2 stacked, or 4 x 8 laid out 4 x 2), or a
-// periphery tile sampled at stride 2 with warps 0-1 (each min(RW, 8) wide), warps 2-7 idle.
-// The Gaussians of the tile's list are staged in shared memory 256 at a time; each thread
-// culls one of them against the warp rectangles, and every warp then walks only its own
-// compacted list, in list order.  The warp shape only changes which pairs are culled (pairs
-// that cannot pass the alpha test), never a pixel's arithmetic.
+struct BlendSmem {
+    float4* p1;
+    float4* p2;
+    float4* p4;
+    float4* rgba;
+    uint32_t* mask;
+    uint8_t (*list)[256];
+};
+
+// Renders one 16x16 work item with the whole 256-thread block: CLS 0 a full-resolution tile with
+// its 8 warps (each RW x 32/RW pixels: 8 x 4 laid out 2 x 4, 16 x 2 stacked, or 4 x 8 laid out
+// 4 x 2); CLS 1 a periphery tile sampled at stride 2 with warps 0-1 (each min(RW, 8) wide); CLS 2
+// a ring-mode quarter tile sampled at stride 4 with lanes 0-15 of warp 0.  The Gaussians of the
+// tile's list are staged in shared memory 256 at a time; each thread culls one of them against
+// the warp rectangles, and every warp then walks only its own compacted list, in list order.
+// The warp shape only changes which pairs are culled (pairs that cannot pass the alpha test),
+// never a pixel's arithmetic.  The tile layout is a compile-time constant of each class.
+template <int K, int RW, int CLS>
+__device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuffers& fb, uint32_t packed,
+                                        const BlendSmem& sm) {
+    constexpr int NT = 256;
+    constexpr int NW = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t lanemask_lt = (1u << lane) - 1u;
+    const int v = static_cast<int>(packed >> 24);
+    const int item = static_cast<int>(packed & (kItemLowres - 1u));
+    const ViewParams& vp = fb.views[v];
+    const FrameStatus& st = fb.status[v];
+    const uint32_t lt = CLS != 0 ? fb.work_low[static_cast<size_t>(v) * fp.max_large + item]
+                            : fb.work_full[static_cast<size_t>(v) * fp.max_large + item];
+    const bool is_fovea = CLS == 0 && static_cast<uint32_t>(item) < st.n_fovea_large;
+    constexpr int S = CLS == 0 ? 1 : CLS == 1 ? kStride : kQuarterStride;
+    // warp rectangle rw x rh (powers of two); warps laid out 2^wx_bits per row
+    constexpr int RW_LOW = RW > 8 ? 8 : RW;  // the periphery sample grid is 8 wide
+    constexpr int RW_BITS = RW == 4 ? 2 : RW == 8 ? 3 : 4, RW_LOW_BITS = RW_LOW == 4 ? 2 : 3;
+    constexpr int rw_bits = CLS == 2 ? 2 : CLS == 1 ? RW_LOW_BITS : RW_BITS;
+    constexpr int rw = 1 << rw_bits, rh = 32 >> rw_bits;
+    constexpr int rh_used = CLS == 2 ? 4 : rh;  // sample rows of a warp that lie in the tile
+    constexpr int wx_bits = CLS == 2 ? 0 : (CLS == 1 ? 3 : 4) - rw_bits;
+    constexpr int n_warps = CLS == 2 ? 1 : CLS == 1 ? 2 : NW;
+    const int ox = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)) * kTileLarge;
+    const int oy = static_cast<int>(lt / static_cast<uint32_t>(vp.glw)) * kTileLarge;
+    const int lx = (warp & ((1 << wx_bits) - 1)) * rw + (lane & (rw - 1));
+    const int ly = (warp >> wx_bits) * rh + (lane >> rw_bits);
+    const int px_i = ox + lx * S, py_i = oy + ly * S;
+    const bool inside = warp < n_warps && (lane >> rw_bits) < rh_used && px_i < vp.width && py_i < vp.height;
+    const float pixel_x = __uint2float_rn(static_cast<uint32_t>(px_i));
+    const float pixel_y = __uint2float_rn(static_cast<uint32_t>(py_i));
+    const uint2 range = fb.ranges[static_cast<size_t>(v) * fp.max_large + lt];
+    const uint32_t* vals = fb.vals[fb.final_buf] + static_cast<size_t>(v) * fp.cap;
+    const float4* rec = fb.rec + 4 * static_cast<size_t>(v) * fp.n_prims;
+
+    float tail_T = 1.0f;
+    float4 tail = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    Frag core[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) { core[k].depth = 3.402823466e+38f; core[k].color = 0u; }
+
+    for (uint32_t start = range.x; start < range.y; start += NT) {
+        const uint32_t n_batch = min(static_cast<uint32_t>(NT), range.y - start);
+        __syncthreads();
+        if (static_cast<uint32_t>(tid) < n_batch && vals[start + tid] >= static_cast<uint32_t>(fp.n_prims)) {
+            sm.mask[tid] = 0u;  // a sentinel slot: no primitive to blend
+        } else if (static_cast<uint32_t>(tid) < n_batch) {
+            const uint32_t p = vals[start + tid];
+            const float4* r = rec + 4 * static_cast<size_t>(p);
+            const float4 P1 = r[0], P2 = r[1], P4 = r[2], c = r[3];
+            sm.p1[tid] = P1;
+            sm.p2[tid] = P2;
+            sm.p4[tid] = P4;
+            sm.rgba[tid] = c;
+            float4 box;
+            bool never;
+            uint32_t m = (1u << n_warps) - 1u;
+            if (cutoff_box(P1, P2, P4, c.w, box, never)) {
+                if (never) m = 0u;
+                else {
+                    Conic q;
+                    const bool ell = cutoff_conic(P1, P2, P4, c.w, q);
+                    m = 0u;
+                    for (int w = 0; w < n_warps; ++w) {
+                        const float ax0 = static_cast<float>(ox + (w & ((1 << wx_bits) - 1)) * rw * S);
+                        const float ax1 = ax0 + static_cast<float>((rw - 1) * S);
+                        const float ay0 = static_cast<float>(oy + (w >> wx_bits) * rh * S);
+                        const float ay1 = ay0 + static_cast<float>((rh_used - 1) * S);
+                        if (box.y >= ax0 && box.x <= ax1 && box.w >= ay0 && box.z <= ay1 &&
+                            (!ell || conic_meets_rect(q, ax0, ax1, ay0, ay1)))
+                            m |= 1u << w;
+                    }
+                }
+            }
+            sm.mask[tid] = m;
+        }
+        __syncthreads();
+        // this warp's list: the batch positions whose mask has its bit, in order
+        int n_mine = 0;
+        for (uint32_t c0 = 0; c0 < n_batch; c0 += 32) {
+            const uint32_t j = c0 + lane;
+            const bool hit = j < n_batch && ((sm.mask[j] >> warp) & 1u);
+            const uint32_t b = __ballot_sync(0xffffffffu, hit);
+            if (hit) sm.list[warp][n_mine + __popc(b & lanemask_lt)] = static_cast<uint8_t>(j);
+            n_mine += __popc(b);
+        }
+        __syncwarp();
+        if (!inside) continue;
+        for (int t = 0; t < n_mine; ++t) {
+            const int j = sm.list[warp][t];
+            const float4 VPMT1 = sm.p1[j], VPMT2 = sm.p2[j], VPMT4 = sm.p4[j];
+            const float4 plane_x = VPMT1 - VPMT4 * pixel_x;
+            const float4 plane_y = VPMT2 - VPMT4 * pixel_y;
+            const float3 nx = xyz(plane_x), ny = xyz(plane_y);
+            const float3 m = plane_x.w * ny - nx * plane_y.w;
+            const float3 d = cross(nx, ny);
+            const float num = dot(m, m);
+            const float den = dot(d, d);
+            // In almost every warp step some lane passes both tests, so the fragment is
+            // evaluated for every lane and the tests only gate its effects (no divergent
+            // exits; a lane that failed cannot contribute: its `frag` is false whatever
+            // rcp/exp return for it).
+            const bool live = !(num > kMaxCutoffSq * den);
+            const float den_rcp = 1.0f / den;
+            const float G = expf(-0.5f * num * den_rcp);
+            const float4 c = sm.rgba[j];
+            const float alpha = fminf(c.w * G, kMaxFragmentAlpha);
+            const bool frag = live && !(alpha < kMinAlpha);
+            float4 pm = make_float4(c.x * alpha, c.y * alpha, c.z * alpha, alpha);
+            // the depth matters only to a fragment that may enter the core (alpha >= 1/20):
+            // evaluated under that test, so that warps whose fragments are all faint skip it
+            float depth = 3.402823466e+38f;
+            if (frag && alpha >= kMinAlphaCore) {
+                const float3 ep = cross(d, m) * den_rcp;
+                depth = dot(xyz(VPMT4), ep) + VPMT4.w;
+            }
+            if (depth < core[K - 1].depth) {
+                Frag f;
+                f.depth = depth;
+                f.color = pack_rgba(pm);
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    if (f.depth < core[k].depth) {
+                        const Frag tf = core[k];
+                        core[k] = f;
+                        f = tf;
+                    }
+                }
+                pm = unpack_rgba(f.color);
+            }
+            if (frag) {
+                const float pt = 1.0f - pm.w;
+                tail += pm;
+                tail_T *= pt;
+            }
+        }
+    }
+    if (inside) {
+        float3 rgb = make_float3(0.0f, 0.0f, 0.0f);
+        float Tc = 1.0f;
+#pragma unroll
+        for (int k = 0; k < K && Tc >= kTransmittanceThreshold; ++k) {
+            const float4 c = unpack_rgba(core[k].color);
+            rgb += Tc * xyz(c);
+            Tc *= 1.0f - c.w;
+        }
+        if (Tc >= kTransmittanceThreshold && tail.w >= kMinAlpha) {
+            const float wt = Tc * (1.0f - tail_T);
+            rgb += wt * (1.0f / tail.w) * xyz(tail);
+        }
+        if (fp.bg_type != 0) {
+            const float wb = Tc * tail_T;
+            if (wb >= kTransmittanceThreshold) {
+                if (fp.bg_type == 1) rgb += wb * eval_sh_background(vp, fp.bg_data, pixel_x, pixel_y);
+                else rgb += wb * eval_tex_background(vp, fp.bg_data, fp.tex_w, fp.tex_h, fp.bg_type == 3, pixel_x, pixel_y);
+            }
+        }
+        float* out = is_fovea ? vp.image : vp.work;
+        store_rgb(out, vp.width, vp.height, px_i, py_i, fp.to_chw != 0, __saturatef(rgb.x), __saturatef(rgb.y),
+                  __saturatef(rgb.z));
+    }
+}
+
+// One persistent kernel blends every tile of every view.  The work list holds the full-resolution
+// tiles, then the periphery tiles, then the quarter tiles, each class heaviest first; blocks take
+// items class by class, each class with its own compiled tile code.
 template <int K, int RW>
 __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FrameParams fp, FrameBuffers fb) {
     constexpr int NT = 256;
@@ -1533,176 +1720,39 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
     __shared__ uint32_t s_mask[NT];
     __shared__ uint8_t s_list[NW][NT];
     __shared__ int s_item;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t lanemask_lt = (1u << lane) - 1u;
-    int total = 0;
-    for (int v = 0; v < fp.n_views; ++v) total += items_of_view(fb.status[v]);
+    const BlendSmem sm{s_p1, s_p2, s_p4, s_rgba, s_mask, s_list};
+    const int tid = threadIdx.x;
+    int n_full = 0, n_half = 0, n_quarter = 0;
+    for (int v = 0; v < fp.n_views; ++v) {
+        const FrameStatus& st = fb.status[v];
+        n_full += static_cast<int>(st.n_fovea_large + st.n_blended_large);
+        n_half += static_cast<int>(st.n_periphery_large);
+        n_quarter += static_cast<int>(st.n_quarter_large);
+    }
     const uint32_t* order = fb.work_order[0];
-    for (;;) {
+    for (;;) {  // full-resolution tiles (listed first)
         if (tid == 0) s_item = static_cast<int>(atomicAdd(&fb.counters[0], 1u));
         __syncthreads();
         const int g = s_item;
         __syncthreads();
-        if (g >= total) break;
-        const uint32_t packed = order[g];
-        const int v = static_cast<int>(packed >> 24);
-        const bool low = (packed & kItemLowres) != 0;
-        const int item = static_cast<int>(packed & (kItemLowres - 1u));
-        const ViewParams& vp = fb.views[v];
-        const FrameStatus& st = fb.status[v];
-        const uint32_t lt = low ? fb.work_low[static_cast<size_t>(v) * fp.max_large + item]
-                                : fb.work_full[static_cast<size_t>(v) * fp.max_large + item];
-        const bool is_fovea = !low && static_cast<uint32_t>(item) < st.n_fovea_large;
-        // ring mode: the quarter tiles follow the periphery tiles in work_low (4 x 4 samples
-        // at stride 4, lanes 0-15 of warp 0)
-        const bool quarter = low && static_cast<uint32_t>(item) >= st.n_periphery_large;
-        const int S = quarter ? kQuarterStride : low ? kStride : 1;
-        // warp rectangle rw x rh (powers of two); warps laid out 2^wx_bits per row
-        constexpr int RW_LOW = RW > 8 ? 8 : RW;  // the periphery sample grid is 8 wide
-        constexpr int RW_BITS = RW == 4 ? 2 : RW == 8 ? 3 : 4, RW_LOW_BITS = RW_LOW == 4 ? 2 : 3;
-        const int rw_bits = quarter ? 2 : low ? RW_LOW_BITS : RW_BITS;
-        const int rw = 1 << rw_bits, rh = 32 >> rw_bits;
-        const int rh_used = quarter ? 4 : rh;  // sample rows of a warp that lie in the tile
-        const int wx_bits = quarter ? 0 : (low ? 3 : 4) - rw_bits;
-        const int n_warps = quarter ? 1 : low ? 2 : NW;
-        const int ox = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)) * kTileLarge;
-        const int oy = static_cast<int>(lt / static_cast<uint32_t>(vp.glw)) * kTileLarge;
-        const int lx = (warp & ((1 << wx_bits) - 1)) * rw + (lane & (rw - 1));
-        const int ly = (warp >> wx_bits) * rh + (lane >> rw_bits);
-        const int px_i = ox + lx * S, py_i = oy + ly * S;
-        const bool inside = warp < n_warps && (lane >> rw_bits) < rh_used && px_i < vp.width && py_i < vp.height;
-        const float pixel_x = __uint2float_rn(static_cast<uint32_t>(px_i));
-        const float pixel_y = __uint2float_rn(static_cast<uint32_t>(py_i));
-        const uint2 range = fb.ranges[static_cast<size_t>(v) * fp.max_large + lt];
-        const uint32_t* vals = fb.vals[fb.final_buf] + static_cast<size_t>(v) * fp.cap;
-        const float4* rec = fb.rec + 4 * static_cast<size_t>(v) * fp.n_prims;
-
-        float tail_T = 1.0f;
-        float4 tail = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        Frag core[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) { core[k].depth = 3.402823466e+38f; core[k].color = 0u; }
-
-        for (uint32_t start = range.x; start < range.y; start += NT) {
-            const uint32_t n_batch = min(static_cast<uint32_t>(NT), range.y - start);
-            __syncthreads();
-            if (static_cast<uint32_t>(tid) < n_batch && vals[start + tid] >= static_cast<uint32_t>(fp.n_prims)) {
-                s_mask[tid] = 0u;  // a sentinel slot: no primitive to blend
-            } else if (static_cast<uint32_t>(tid) < n_batch) {
-                const uint32_t p = vals[start + tid];
-                const float4* r = rec + 4 * static_cast<size_t>(p);
-                const float4 P1 = r[0], P2 = r[1], P4 = r[2], c = r[3];
-                s_p1[tid] = P1;
-                s_p2[tid] = P2;
-                s_p4[tid] = P4;
-                s_rgba[tid] = c;
-                float4 box;
-                bool never;
-                uint32_t m = (1u << n_warps) - 1u;
-                if (cutoff_box(P1, P2, P4, c.w, box, never)) {
-                    if (never) m = 0u;
-                    else {
-                        Conic q;
-                        const bool ell = cutoff_conic(P1, P2, P4, c.w, q);
-                        m = 0u;
-                        for (int w = 0; w < n_warps; ++w) {
-                            const float ax0 = static_cast<float>(ox + (w & ((1 << wx_bits) - 1)) * rw * S);
-                            const float ax1 = ax0 + static_cast<float>((rw - 1) * S);
-                            const float ay0 = static_cast<float>(oy + (w >> wx_bits) * rh * S);
-                            const float ay1 = ay0 + static_cast<float>((rh_used - 1) * S);
-                            if (box.y >= ax0 && box.x <= ax1 && box.w >= ay0 && box.z <= ay1 &&
-                                (!ell || conic_meets_rect(q, ax0, ax1, ay0, ay1)))
-                                m |= 1u << w;
-                        }
-                    }
-                }
-                s_mask[tid] = m;
-            }
-            __syncthreads();
-            // this warp's list: the batch positions whose mask has its bit, in order
-            int n_mine = 0;
-            for (uint32_t c0 = 0; c0 < n_batch; c0 += 32) {
-                const uint32_t j = c0 + lane;
-                const bool hit = j < n_batch && ((s_mask[j] >> warp) & 1u);
-                const uint32_t b = __ballot_sync(0xffffffffu, hit);
-                if (hit) s_list[warp][n_mine + __popc(b & lanemask_lt)] = static_cast<uint8_t>(j);
-                n_mine += __popc(b);
-            }
-            __syncwarp();
-            if (!inside) continue;
-            for (int t = 0; t < n_mine; ++t) {
-                const int j = s_list[warp][t];
-                const float4 VPMT1 = s_p1[j], VPMT2 = s_p2[j], VPMT4 = s_p4[j];
-                const float4 plane_x = VPMT1 - VPMT4 * pixel_x;
-                const float4 plane_y = VPMT2 - VPMT4 * pixel_y;
-                const float3 nx = xyz(plane_x), ny = xyz(plane_y);
-                const float3 m = plane_x.w * ny - nx * plane_y.w;
-                const float3 d = cross(nx, ny);
-                const float num = dot(m, m);
-                const float den = dot(d, d);
-                // In almost every warp step some lane passes both tests, so the fragment is
-                // evaluated for every lane and the tests only gate its effects (no divergent
-                // exits; a lane that failed cannot contribute: its `frag` is false whatever
-                // rcp/exp return for it).
-                const bool live = !(num > kMaxCutoffSq * den);
-                const float den_rcp = 1.0f / den;
-                const float G = expf(-0.5f * num * den_rcp);
-                const float4 c = s_rgba[j];
-                const float alpha = fminf(c.w * G, kMaxFragmentAlpha);
-                const bool frag = live && !(alpha < kMinAlpha);
-                float4 pm = make_float4(c.x * alpha, c.y * alpha, c.z * alpha, alpha);
-                // the depth matters only to a fragment that may enter the core (alpha >= 1/20):
-                // evaluated under that test, so that warps whose fragments are all faint skip it
-                float depth = 3.402823466e+38f;
-                if (frag && alpha >= kMinAlphaCore) {
-                    const float3 ep = cross(d, m) * den_rcp;
-                    depth = dot(xyz(VPMT4), ep) + VPMT4.w;
-                }
-                if (depth < core[K - 1].depth) {
-                    Frag f;
-                    f.depth = depth;
-                    f.color = pack_rgba(pm);
-#pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        if (f.depth < core[k].depth) {
-                            const Frag tf = core[k];
-                            core[k] = f;
-                            f = tf;
-                        }
-                    }
-                    pm = unpack_rgba(f.color);
-                }
-                if (frag) {
-                    const float pt = 1.0f - pm.w;
-                    tail += pm;
-                    tail_T *= pt;
-                }
-            }
-        }
-        if (inside) {
-            float3 rgb = make_float3(0.0f, 0.0f, 0.0f);
-            float Tc = 1.0f;
-#pragma unroll
-            for (int k = 0; k < K && Tc >= kTransmittanceThreshold; ++k) {
-                const float4 c = unpack_rgba(core[k].color);
-                rgb += Tc * xyz(c);
-                Tc *= 1.0f - c.w;
-            }
-            if (Tc >= kTransmittanceThreshold && tail.w >= kMinAlpha) {
-                const float wt = Tc * (1.0f - tail_T);
-                rgb += wt * (1.0f / tail.w) * xyz(tail);
-            }
-            if (fp.bg_type != 0) {
-                const float wb = Tc * tail_T;
-                if (wb >= kTransmittanceThreshold) {
-                    if (fp.bg_type == 1) rgb += wb * eval_sh_background(vp, fp.bg_data, pixel_x, pixel_y);
-                    else rgb += wb * eval_tex_background(vp, fp.bg_data, fp.tex_w, fp.tex_h, fp.bg_type == 3, pixel_x, pixel_y);
-                }
-            }
-            float* out = is_fovea ? vp.image : vp.work;
-            store_rgb(out, vp.width, vp.height, px_i, py_i, fp.to_chw != 0, __saturatef(rgb.x), __saturatef(rgb.y),
-                      __saturatef(rgb.z));
-        }
+        if (g >= n_full) break;
+        blend_tile<K, RW, 0>(fp, fb, order[g], sm);
+    }
+    for (;;) {  // periphery tiles
+        if (tid == 0) s_item = static_cast<int>(atomicAdd(&fb.counters[1], 1u));
+        __syncthreads();
+        const int g = s_item;
+        __syncthreads();
+        if (g >= n_half) break;
+        blend_tile<K, RW, 1>(fp, fb, order[n_full + g], sm);
+    }
+    for (;;) {  // ring-mode quarter tiles
+        if (tid == 0) s_item = static_cast<int>(atomicAdd(&fb.counters[2], 1u));
+        __syncthreads();
+        const int g = s_item;
+        __syncthreads();
+        if (g >= n_quarter) break;
+        blend_tile<K, RW, 2>(fp, fb, order[n_full + n_half + g], sm);
     }
 }
 

@@ -148,10 +148,11 @@ struct FrameBuffers {
     uint32_t* sort_ticket;    // [V][kSortMaxPasses] tiles handed out so far
 };
 
-// Work ordering: tiles are bucketed by list length in quarter octaves and blended in
-// descending bucket order, so that the longest lists start first (longest-processing-time
-// scheduling of the persistent blend blocks).
-constexpr int kOrderBuckets = 130;
+// Work ordering: tiles are bucketed by class and by list length in quarter octaves and
+// blended in descending bucket order: full-resolution tiles, then periphery, then quarter
+// tiles, the longest lists of each class first (longest-processing-time scheduling).
+constexpr int kCostBuckets = 130;                     // per tile class
+constexpr int kOrderBuckets = 3 * kCostBuckets;       // full-resolution, periphery, quarter
 constexpr int kCounterWords = 4 + 2 * kOrderBuckets;  // counters, histogram, cursors
 
 // Launchers exported by each math flavour (fast = -use_fast_math, ieee = default).
