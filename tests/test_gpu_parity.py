@@ -272,6 +272,21 @@ def test_large_footprints_use_cooperative_emission(renderer):
     assert psnr(img, _oracle_image(g, v, K=8, active_sh_bases=1)) >= REF_PSNR_DB
 
 
+def test_wide_grid_uses_32bit_keys_and_three_sort_passes(renderer):
+    """4400 x 4200: 72,325 large tiles, so stored keys are 32-bit with 17 significant bits
+    (three onesweep passes) and the reference's keys 19-bit; instances exact vs the oracle."""
+    g = scene.make_gaussians(20000, 0, seed=9)
+    v = scene.make_view(4400, 4200, position=(0.0, 0.0, -4.5), gaze_ndc=(0.2, -0.1))
+    st = [F.settings_from_view(v, K=8, active_sh_bases=1)]
+    img = renderer.render(*F.gaussians_to_torch(g), st, fast_math=False)[0].cpu().numpy()
+    m = renderer.intermediates(0)
+    geo = O.geometry(v)
+    assert geo["grid_large_w"] * geo["grid_large_h"] > 65536 and geo["end_bit"] > 16
+    oi = O.instances(v, m["n_touched"], m["screen_bounds"])
+    assert_instances_equal(m, oi, geo["end_bit"], "32-bit keys")
+    assert psnr(img, _oracle_image(g, v, K=8, active_sh_bases=1)) >= REF_PSNR_DB
+
+
 def test_capacity_overflow_grows_and_rerenders():
     r = F.Renderer("cuda:0")
     try:
