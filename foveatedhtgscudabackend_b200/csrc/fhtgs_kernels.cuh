@@ -1657,24 +1657,23 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
             float4 pm = make_float4(c.x * alpha, c.y * alpha, c.z * alpha, alpha);
             // the depth matters only to a fragment that may enter the core (alpha >= 1/20):
             // evaluated under that test, so that warps whose fragments are all faint skip it
-            float depth = 3.402823466e+38f;
             if (frag && alpha >= kMinAlphaCore) {
                 const float3 ep = cross(d, m) * den_rcp;
-                depth = dot(xyz(VPMT4), ep) + VPMT4.w;
-            }
-            if (depth < core[K - 1].depth) {
-                Frag f;
-                f.depth = depth;
-                f.color = pack_rgba(pm);
+                const float depth = dot(xyz(VPMT4), ep) + VPMT4.w;
+                if (depth < core[K - 1].depth) {
+                    Frag f;
+                    f.depth = depth;
+                    f.color = pack_rgba(pm);
 #pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    if (f.depth < core[k].depth) {
-                        const Frag tf = core[k];
-                        core[k] = f;
-                        f = tf;
+                    for (int k = 0; k < K; ++k) {
+                        if (f.depth < core[k].depth) {
+                            const Frag tf = core[k];
+                            core[k] = f;
+                            f = tf;
+                        }
                     }
+                    pm = unpack_rgba(f.color);
                 }
-                pm = unpack_rgba(f.color);
             }
             if (frag) {
                 const float pt = 1.0f - pm.w;
