@@ -277,7 +277,7 @@ def run_ours(a, world, rank, local):
     # stream while step k+1 renders (two pinned output buffers); the timed region ends after the
     # last copy has landed.
     e2e = None
-    e2e_steps = 0 if a.no_e2e else (a.e2e_steps or max(3, min(a.steps, 10)))
+    e2e_steps = 0 if a.no_e2e else (a.e2e_steps or max(3, a.steps))
     # the per-frame inputs of both eyes (camera matrices, masks, area tables) packed into one
     # pinned host buffer, so that each step moves them with a single host->device copy; the
     # settings read device views of the packed copy (gaze stays a host value)
@@ -304,16 +304,18 @@ def run_ours(a, world, rank, local):
     copy_stream = torch.cuda.Stream(dev)
     copy_done = [torch.cuda.Event(), torch.cuda.Event()]
 
-    def e2e_step(k: int):
+    dev_imgs = [[torch.empty((3, v.height, v.width), device=dev) for v in (left, right)] for _ in range(2)]
+
+    def e2e_step(k: int, dropin: bool):
         cur = torch.cuda.current_stream(dev)
+        buf = k % 2
+        copy_done[buf].synchronize()  # the copy that used these buffers two steps ago has landed
         dev_pack.copy_(host_pack, non_blocking=True)
         sd = sd_packed
-        if a.foveation == "reference":
+        if dropin and a.foveation == "reference":  # the reference's call: blocking, fresh images
             a_img, b_img = _C_stereo.render(*gt, *sd[0].as_tuple(), *sd[1].as_tuple(), True, False, False)
-        else:  # the drop-in call has only the reference's foveation: the Renderer, blocking
-            a_img, b_img = r.render(*gt, sd, to_chw=True, fast_math=True, sync=True)
-        buf = k % 2
-        copy_done[buf].synchronize()  # the copy that used this pinned buffer two steps ago
+        else:  # the C ABI's asynchronous frame (fhtgs_render_views) into double-buffered images
+            a_img, b_img = r.render(*gt, sd, to_chw=True, fast_math=True, images=dev_imgs[buf], sync=dropin)
         copy_stream.wait_stream(cur)
         with torch.cuda.stream(copy_stream):
             out_host[buf][0].copy_(a_img, non_blocking=True)
@@ -322,26 +324,34 @@ def run_ours(a, world, rank, local):
             b_img.record_stream(copy_stream)
             copy_done[buf].record(copy_stream)
 
-    if e2e_steps > 0:
+    def e2e_run(dropin: bool) -> float:
         for k in range(2):
-            e2e_step(k)
+            e2e_step(k, dropin)
         torch.cuda.synchronize(dev)
         barrier(world)
         t0 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         for k in range(e2e_steps):
-            e2e_step(k)
+            e2e_step(k, dropin)
         stream.wait_stream(copy_stream)
         t1 = torch.cuda.Event(enable_timing=True)
         t1.record(stream)
         torch.cuda.synchronize(dev)
-        e2e_ms = max_over_ranks(t0.elapsed_time(t1), world)
+        if any(r.frame_info(i)["overflow"] for i in range(2)):
+            raise RuntimeError("instance capacity overflow inside the end-to-end region")
+        return max_over_ranks(t0.elapsed_time(t1), world)
+
+    if e2e_steps > 0:
+        e2e_ms = e2e_run(dropin=False)
+        dropin_ms = e2e_run(dropin=True)
         e2e = {"value": round(world * e2e_steps / (e2e_ms / 1000.0), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
-               "api": "foveatedhtgscudabackend_b200._C_stereo.render" if a.foveation == "reference"
-               else "foveatedhtgscudabackend_b200.Renderer.render (blocking)",
+               "api": "foveatedhtgscudabackend_b200.Renderer.render(sync=False) -> fhtgs_render_views (asynchronous)",
                "steps": e2e_steps, "h2d": "one packed copy of both eyes' inputs per step",
-               "d2h": "double-buffered pinned copies on a copy stream"}
+               "d2h": "double-buffered pinned copies on a copy stream",
+               "dropin_value": round(world * e2e_steps / (dropin_ms / 1000.0), 3),
+               "dropin_api": "foveatedhtgscudabackend_b200._C_stereo.render (blocking, as the reference's call)"
+               if a.foveation == "reference" else "foveatedhtgscudabackend_b200.Renderer.render(sync=True)"}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
