@@ -799,15 +799,18 @@ __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParam
         if (cnt <= kSeqTiles) {
             uint64_t w = off;
             const uint64_t end = static_cast<uint64_t>(off) + nv;
-            for (uint32_t k = 0; k < cnt && w < end; ++k) {
-                const uint32_t tile = (b.z + k / bw) * glw + b.x + k % bw;
-                if (!tile_visible(vp.vis_mask, tile)) continue;
-                if (w < lim) {
-                    keys[w] = static_cast<KeyT>(tile);
-                    vals[w] = static_cast<uint32_t>(i);
-                    if (onesweep) count_key(s_dhist, passes, tile);
+            for (uint32_t ty = b.z; ty < b.w && w < end; ++ty) {  // row-major over the bounds
+                const uint32_t row = ty * glw;
+                for (uint32_t tx = b.x; tx < b.y && w < end; ++tx) {
+                    const uint32_t tile = row + tx;
+                    if (!tile_visible(vp.vis_mask, tile)) continue;
+                    if (w < lim) {
+                        keys[w] = static_cast<KeyT>(tile);
+                        vals[w] = static_cast<uint32_t>(i);
+                        if (onesweep) count_key(s_dhist, passes, tile);
+                    }
+                    ++w;
                 }
-                ++w;
             }
             // a visibility area table that counts more tiles than the mask holds leaves slots
             // over: they get sentinels that the range and blend stages skip
