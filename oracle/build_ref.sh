@@ -63,12 +63,18 @@ build_module() {
 
 MODS=("$@"); [ ${#MODS[@]} -eq 0 ] && MODS=(_C _C_benchmarking _C_stereo _C_visualization)
 RS="$FHB/rasterization/src"; TB="$FHB/torch_bindings"
+# the modules are independent: build them side by side (about 3 GB of host memory each)
+pids=()
 for m in "${MODS[@]}"; do
   case $m in
-    _C) build_module _C 0 "$TB/bindings.cpp" "$RS/inference_api.cu" "$RS/inference.cu" "$RS/utils/torch_utils.cpp" ;;
-    _C_benchmarking) build_module _C_benchmarking 1 "$TB/bindings_benchmarking.cpp" "$RS/fast_inference_api.cu" "$RS/inference.cu" "$RS/utils/torch_utils.cpp" ;;
-    _C_stereo) build_module _C_stereo 1 "$TB/bindings_stereo.cpp" "$RS/inference_stereo_api.cu" "$RS/inference_stereo.cu" "$RS/utils/torch_utils.cpp" ;;
-    _C_visualization) build_module _C_visualization 1 "$TB/bindings_visualization.cpp" "$FHB/visualization/src/visualization_api.cu" "$FHB/visualization/src/visualization.cu" "$RS/utils/torch_utils.cpp" ;;
+    _C) build_module _C 0 "$TB/bindings.cpp" "$RS/inference_api.cu" "$RS/inference.cu" "$RS/utils/torch_utils.cpp" & ;;
+    _C_benchmarking) build_module _C_benchmarking 1 "$TB/bindings_benchmarking.cpp" "$RS/fast_inference_api.cu" "$RS/inference.cu" "$RS/utils/torch_utils.cpp" & ;;
+    _C_stereo) build_module _C_stereo 1 "$TB/bindings_stereo.cpp" "$RS/inference_stereo_api.cu" "$RS/inference_stereo.cu" "$RS/utils/torch_utils.cpp" & ;;
+    _C_visualization) build_module _C_visualization 1 "$TB/bindings_visualization.cpp" "$FHB/visualization/src/visualization_api.cu" "$FHB/visualization/src/visualization.cu" "$RS/utils/torch_utils.cpp" & ;;
     *) echo "unknown module $m" >&2; exit 2 ;;
   esac
+  pids+=($!)
 done
+status=0
+for p in "${pids[@]}"; do wait "$p" || status=1; done
+exit $status

@@ -270,3 +270,28 @@ def test_server_outputs_are_recycled(scenes):
             srv.release(cs[0].ticket)  # released twice
     # the second round finds every output buffer and table in the pool: nothing new is held
     assert len(set(sizes[len(reqs):])) == 1 and sizes[-1] == sizes[len(reqs) - 1]
+
+
+def test_ring_foveation_scenes_match_the_renderer(scenes):
+    """A scene registered with ring foveation is served exactly as Renderer renders it."""
+    gt, active = scenes[0]
+    reqs = make_requests(4, 1, seed=21)
+    r = F.Renderer(DEV)
+    r.set_foveation("rings", 0.2, 0.5)
+    ref = []
+    for _, eyes in reqs:
+        st = [F.settings_from_view(v, K=8, active_sh_bases=active, device=DEV) for v in eyes]
+        ref.append([x.clone() for x in r.render(*gt, st, fast_math=True)])
+    r.close()
+    with Server(DEV, max_in_flight=2, max_batch_requests=4) as srv:
+        sid = srv.add_scene(*gt, K=8, active_sh_bases=active, foveation="rings", rings=(0.2, 0.5))
+        srv.pause()
+        for k, (_, eyes) in enumerate(reqs):
+            srv.submit(sid, eyes, tag=k)
+        srv.resume()
+        srv.drain(timeout_ms=30000)
+        comps = srv.poll()
+        assert len(comps) == len(reqs) and all(c.ok for c in comps)
+        for c in comps:
+            for e in range(2):
+                assert torch.equal(c.images[e], ref[c.tag][e]), f"request {c.tag} eye {e}"
