@@ -1039,6 +1039,19 @@ __device__ __forceinline__ void st_look(uint32_t* p, uint32_t v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Lanes of the warp whose 8-bit digit equals this lane's (the mask __match_any_sync returns),
+// from eight ballots over the digit bits; lanes without an item (ok false) match no lane.
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok) {
+    uint32_t peers = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+    for (int b = 0; b < kSortRadixBits; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t m = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? m : ~m;
+    }
+    return peers;
+}
+
 template <typename KeyT, int ITEMS>
 __global__ void __launch_bounds__(kSortThreads, 3) sort_onesweep_kernel(FrameParams fp, FrameBuffers fb, int buf, int pass) {
     constexpr int TILE = kSortThreads * ITEMS;
@@ -1083,7 +1096,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_onesweep_kernel(FramePar
     for (int it = 0; it < ITEMS; ++it) {
         const bool ok = wbase + it * 32 < n_here;
         const uint32_t d = ok ? (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1) : kSortBins;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t peers = digit_peers(d, ok);
         const uint32_t base = ok ? s_whist[warp][d] : 0u;
         __syncwarp();
         rank[it] = base + __popc(peers & lanemask_lt);
