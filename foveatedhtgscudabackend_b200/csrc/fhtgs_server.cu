@@ -181,14 +181,22 @@ void reap_locked(fhtgs_server_s* S) {
         any = true;
         Scene& sc = S->scenes[sl.scene];
         unsigned long long need = 0;
-        for (int v = 0; v < sl.n_views; ++v) need = std::max(need, sl.h_status[v].n_instances);
+        bool failed = false;  // a bounded device wait gave up (sort look-back, attribute staging)
+        for (int v = 0; v < sl.n_views; ++v) {
+            need = std::max(need, sl.h_status[v].n_instances);
+            failed = failed || (sl.h_status[v].overflow & (kFrameErrSortLookback | kFrameErrStaging)) != 0;
+        }
         const bool overflow = need > static_cast<unsigned long long>(sl.cap);
         const int64_t grown = static_cast<int64_t>(need + need / 4);
         if (grown > sc.cap_need) sc.cap_need = grown;
         --sc.in_flight;
         ++S->stats.frames;
         S->stats.views += sl.n_views;
-        if (overflow) {
+        if (failed) {
+            for (const Pending& p : sl.batch)
+                complete_locked(S, p, FHTGS_ERR_CUDA, sl.n_views, sl.t_done,
+                                "a bounded device wait of the frame gave up (sort look-back or attribute staging)");
+        } else if (overflow) {
             ++S->stats.retries;
             for (auto it = sl.batch.rbegin(); it != sl.batch.rend(); ++it) {
                 Pending p = *it;
