@@ -594,6 +594,8 @@ fhtgs_status fhtgs_get_frame_info(fhtgs_context ctx, int32_t view, fhtgs_frame_i
     fhtgs_status st = read_status(ctx);
     if (st != FHTGS_OK) return st;
     const FrameStatus& s = ctx->h_status[view];
+    if (s.overflow & (kFrameErrSortLookback | kFrameErrStaging))
+        return fail(FHTGS_ERR_CUDA, "the frame is incomplete: a bounded device wait gave up (sort look-back or attribute staging)");
     // the reference's count has a meaning only in its own foveation layout
     out->n_instances = static_cast<int64_t>(ctx->fp.fov_mode == kFoveationReference ? s.n_instances_ref : s.n_instances);
     out->instance_capacity = ctx->fp.cap;

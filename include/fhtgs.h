@@ -189,6 +189,9 @@ fhtgs_status fhtgs_render_views(fhtgs_context ctx, const fhtgs_primitives* prims
 fhtgs_status fhtgs_render_views_sync(fhtgs_context ctx, const fhtgs_primitives* prims,
                                      const fhtgs_view* views, int32_t n_views,
                                      const fhtgs_settings* settings, void* stream);
+/* Waits for the last frame and reports one view of it.  FHTGS_ERR_CUDA if the frame is
+ * incomplete because one of its bounded device-side waits gave up (the sort's look-back over
+ * earlier tiles, or the preprocess's bulk-copy barrier). */
 fhtgs_status fhtgs_get_frame_info(fhtgs_context ctx, int32_t view, fhtgs_frame_info* out);
 fhtgs_status fhtgs_copy_intermediates(fhtgs_context ctx, int32_t view, fhtgs_intermediates* out);
 
