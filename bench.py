@@ -82,10 +82,11 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--cpu-budget-s", type=float, default=30.0, help="upper bound of the CPU baseline sample")
-    ap.add_argument("--workload", choices=["stereo", "batched", "precision", "served"], default="stereo",
+    ap.add_argument("--workload", choices=["stereo", "batched", "precision", "served", "plain"], default="stereo",
                     help="stereo: the headline stereo frame; batched: 64 mixed-resolution cameras of a 3M scene; "
                          "precision: 6M-Gaussian stereo frame with fp16/bf16 attribute storage; served: a Poisson "
-                         "stream of stereo requests against 3 resident scenes through the request server")
+                         "stream of stereo requests against 3 resident scenes through the request server; plain: "
+                         "100k SH0 Gaussians, one 1280x720 view, K=4, no foveation")
     ap.add_argument("--n-views", type=int, default=64, help="cameras per batch (batched workload)")
     ap.add_argument("--duration", type=float, default=10.0, help="seconds of arrivals (served workload)")
     ap.add_argument("--rate", type=float, default=240.0, help="request arrivals per second (served workload)")
@@ -391,6 +392,75 @@ def run_ours(a, world, rank, local):
 
 
 # ------------------------------------------------------------------------------------------
+# plain single view: 100k Gaussians SH0, 1280x720, K = 4, no foveation
+# ------------------------------------------------------------------------------------------
+def run_plain(a, world, rank, local):
+    """100k Gaussians (SH degree 0, seed 0), one 1280x720 view from z = -6, K = 4, no
+    foveation (every tile at full resolution; the reference cannot switch its foveation off).
+    `value` = frames/s replaying a captured frame graph; beside it the eager frame and one
+    blocking drop-in `_C_benchmarking.benchmark` call per frame in the reference's own layout."""
+    import torch
+
+    import foveatedhtgscudabackend_b200 as F
+    from foveatedhtgscudabackend_b200 import _C_benchmarking, scene
+
+    dev = torch.device("cuda", local)
+    n = a.n_gaussians if a.n_gaussians != 1_000_000 else 100_000
+    g = scene.make_gaussians(n, 0, seed=0)
+    v = scene.make_view(1280, 720)
+    gt = F.gaussians_to_torch(g, dev)
+    st = [F.settings_from_view(v, K=4, active_sh_bases=1, device=dev)]
+    stream = torch.cuda.current_stream(dev)
+    r = F.Renderer(dev)
+    r.set_foveation(a.foveation if a.foveation != "reference" else "none", *a.rings)
+    img = [torch.empty((3, v.height, v.width), device=dev)]
+    r.render(*gt, st, images=img, sync=True)
+    graph = r.capture(*gt, st, images=img, capacity_headroom=1.1)
+    steps = max(a.steps, 200)
+
+    def timed(fn):
+        for _ in range(max(a.warmup, 3)):
+            fn()
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        ev[0].record(stream)
+        for k in range(steps):
+            fn()
+            ev[k + 1].record(stream)
+        torch.cuda.synchronize(dev)
+        per = sorted(ev[k].elapsed_time(ev[k + 1]) for k in range(steps))
+        return max_over_ranks(ev[0].elapsed_time(ev[steps]), world), per
+
+    launches0 = r.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    graph_ms, per = timed(graph.launch)
+    clk = clocks.stop()
+    launches = r.launch_count() - launches0
+    eager_ms, _ = timed(lambda: r.render(*gt, st, images=img, sync=False))
+    graph.close()
+    ref_layout_ms, _ = timed(lambda: _C_benchmarking.benchmark(*gt, *st[0].as_tuple(), True, False, False))
+    r.close()
+    if rank != 0:
+        return None
+    fov = a.foveation if a.foveation != "reference" else "none"
+    return {
+        "metric": "plain single-view frames/s (captured frame graph)", "value": round(world * steps / (graph_ms / 1000.0), 2),
+        "unit": "frames/s", "n_gpus": world, "steps": steps, "warmup": max(a.warmup, 3),
+        "ms_per_step": round(graph_ms / steps, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"plain_{n // 1000}k_sh0_1280x720_k4_{fov}", "n_gaussians": n, "sh_degree": 0,
+                   "view": "1280x720 from z = -6", "K": 4, "foveation": FOVEATION_TEXT[fov].format(*a.rings),
+                   "l2": "scene and image fit in L2 (small config)"},
+        "latency_ms": {"p50": round(float(np.percentile(per, 50)), 4), "p99": round(float(np.percentile(per, 99)), 4)},
+        "eager_frames_per_s": round(world * steps / (eager_ms / 1000.0), 2),
+        "dropin_reference_layout_frames_per_s": round(world * steps / (ref_layout_ms / 1000.0), 2),
+        "gpu_launches": int(launches), "clocks": clk,
+    }
+
+
+# ------------------------------------------------------------------------------------------
 # batched workload: many cameras of uneven resolution and gaze per frame
 # ------------------------------------------------------------------------------------------
 def run_batched(a, world, rank, local):
@@ -426,11 +496,17 @@ def run_batched(a, world, rank, local):
         per = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
         return max_over_ranks(ev[0].elapsed_time(ev[steps]), world), per
 
+    # per view 1-3 foveation regions (seeded): 1 = every tile at full resolution; 2 = full
+    # resolution within NDC radius 0.15 of the gaze, 2x down beyond; 3 = full / 2x within 0.4 /
+    # 4x beyond (the rings of the stereo config)
+    rng = np.random.default_rng(rank + 4242)
+    rings = [int(x) for x in rng.integers(1, 4, size=len(views))]
+    vf = [{1: "none", 2: ("rings", 0.15, 100.0), 3: ("rings", 0.15, 0.4)}[c] for c in rings]
     r = F.Renderer(dev)
     imgs = [torch.empty((3, v.height, v.width), device=dev) for v in views]
-    r.render(*gt, st, images=imgs, sync=True)
-    tuning = r.autotune(*gt, st, repeats=2)
-    graph = r.capture(*gt, st, images=imgs, capacity_headroom=1.1)
+    r.render(*gt, st, images=imgs, sync=True, view_foveation=vf)
+    tuning = r.autotune(*gt, st, repeats=2, view_foveation=vf)
+    graph = r.capture(*gt, st, images=imgs, capacity_headroom=1.1, view_foveation=vf)
     for _ in range(max(a.warmup, 0)):
         graph.launch()
     launches0 = r.launch_count()
@@ -440,15 +516,19 @@ def run_batched(a, world, rank, local):
     clk = clocks.stop()
     launches = r.launch_count() - launches0
     overflow = any(r.frame_info(i)["overflow"] for i in range(len(st)))
-    eager_ms, _ = timed(lambda: r.render(*gt, st, images=imgs, sync=False), a.steps)
+    eager_ms, _ = timed(lambda: r.render(*gt, st, images=imgs, sync=False, view_foveation=vf), a.steps)
     graph.close()
-    r.close()
-    # plain per-request path: one blocking drop-in call per view
+    # plain per-request path: one blocking call per view, each with its own foveation
+    rp = F.Renderer(dev)
     plain_steps = max(1, min(a.steps, 3))
-    for s in st[:4]:
-        _C_benchmarking.benchmark(*gt, *s.as_tuple(), True, False, False)
-    plain_ms, _ = timed(lambda: [_C_benchmarking.benchmark(*gt, *s.as_tuple(), True, False, False) for s in st],
-                        plain_steps)
+
+    def plain_frame():
+        for s_, f_ in zip(st, vf):
+            rp.render(*gt, [s_], sync=True, view_foveation=[f_])
+    plain_frame()
+    plain_ms, _ = timed(plain_frame, plain_steps)
+    rp.close()
+    r.close()
     if rank != 0:
         return None
     nv = len(st)
@@ -462,11 +542,14 @@ def run_batched(a, world, rank, local):
                    "views": nv, "megapixels_per_batch": round(pixels / 1e6, 2),
                    "resolutions": "uniform from 640x480, 1280x720, 1920x1080, 2064x2208",
                    "cameras": "sphere r in [4, 8] looking at the origin, gaze uniform in [-0.8, 0.8]^2 NDC",
-                   "foveation": "reference constants (one fovea ring + blend band + 2x-down periphery)",
+                   "foveation": "per view 1-3 regions: all full / full r<0.15 + 2x / full r<0.15, 2x r<0.4, 4x "
+                                "(seeded; counts per view in `view_regions`)",
                    "l2": "inputs larger than L2"},
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p99": round(float(np.percentile(lat, 99)), 3)},
         "eager_batch_views_per_s": round(world * a.steps * nv / (eager_ms / 1000.0), 2),
         "plain_per_view_views_per_s": round(world * plain_steps * nv / (plain_ms / 1000.0), 2),
+        "plain_per_view_api": "Renderer.render(sync=True), one blocking call per view (the drop-in has only the reference's foveation)",
+        "view_regions": rings,
         "tuning": tuning, "overflow": overflow, "gpu_launches": int(launches), "clocks": clk,
     }
 
@@ -750,6 +833,8 @@ def main(argv=None) -> int:
             line = run_precision(a, world, rank, local)
         elif a.workload == "served":
             line = run_served(a, world, rank, local)
+        elif a.workload == "plain":
+            line = run_plain(a, world, rank, local)
         else:
             line = run_ours(a, world, rank, local)
         if line is not None:

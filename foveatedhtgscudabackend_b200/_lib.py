@@ -52,7 +52,7 @@ class View(C.Structure):
     _fields_ = [("M", vp), ("VPM", vp), ("VPR_inv", vp), ("cam_position", vp), ("gaze_x", c_f), ("gaze_y", c_f),
                 ("visibility_mask", vp), ("visibility_mask_area_table", vp), ("fovea_mask_area_table", vp),
                 ("width", c_i32), ("height", c_i32), ("focal_x", c_f), ("focal_y", c_f), ("center_x", c_f),
-                ("center_y", c_f), ("image", vp)]
+                ("center_y", c_f), ("image", vp), ("foveation", c_i32), ("ring_full", c_f), ("ring_half", c_f)]
 
 
 class Settings(C.Structure):

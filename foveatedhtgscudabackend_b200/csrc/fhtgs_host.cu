@@ -94,6 +94,7 @@ struct fhtgs_context_s {
     FrameBuffers fb{};
     std::vector<ViewGeom> geo;
     std::vector<fhtgs_view> views;
+    int frame_foveation = 0;          // the settings' foveation of the last frame
     cudaStream_t stream = nullptr;
     // profiling: events around the stages of the last frame, and a launch counter
     bool profile = false;
@@ -206,6 +207,13 @@ fhtgs_status validate(const fhtgs_primitives* p, const fhtgs_view* views, int n_
         if (!v.M || !v.VPM || !v.VPR_inv || !v.cam_position || !v.visibility_mask || !v.visibility_mask_area_table ||
             !v.fovea_mask_area_table || !v.image)
             return fail(FHTGS_ERR_INVALID_ARGUMENT, "null view pointer");
+        if (v.foveation < 0 || v.foveation > FHTGS_FOVEATION_NONE + 1)
+            return fail(FHTGS_ERR_INVALID_ARGUMENT, "unknown per-view foveation");
+        if (v.foveation == FHTGS_FOVEATION_RINGS + 1) {
+            if (!(v.ring_full >= 0.0f) || !(v.ring_half >= v.ring_full) || !std::isfinite(v.ring_half))
+                return fail(FHTGS_ERR_INVALID_ARGUMENT, "view ring radii must satisfy 0 <= ring_full <= ring_half < inf");
+            if (s->blur_periphery) return fail(FHTGS_ERR_INVALID_ARGUMENT, "blur_periphery is not available with ring foveation");
+        }
     }
     return FHTGS_OK;
 }
@@ -292,9 +300,6 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     fp.n_blocks_prim = nbp;
     fp.blend_rw = ctx->tuning.blend_warp_width;
     fp.blend_blocks = ctx->tuning.blend_blocks_per_sm;
-    fp.fov_mode = s->foveation;
-    fp.ring_full2 = s->ring_full * s->ring_full;
-    fp.ring_half2 = s->ring_half * s->ring_half;
 
     FrameBuffers fb{};
     fb.views = reinterpret_cast<ViewParams*>(A + L.off_views);
@@ -359,6 +364,12 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
         p.fovea_sat = v.fovea_mask_area_table;
         p.image = v.image;
         p.work = s->blur_periphery ? reinterpret_cast<float*>(A + L.temp_offsets[i]) : v.image;
+        // foveation: the view's own when it sets one, else the frame's
+        const bool own = v.foveation > 0;
+        const float rf = own ? v.ring_full : s->ring_full, rh = own ? v.ring_half : s->ring_half;
+        p.fov_mode = own ? v.foveation - 1 : s->foveation;
+        p.ring_full2 = rf * rf;
+        p.ring_half2 = rh * rh;
     }
     Gaussians gs{prims->positions, prims->scales, prims->rotations, prims->opacities, prims->sh_0, prims->sh_rest,
                  prims->storage == FHTGS_STORAGE_HALF ? 1 : 0};
@@ -400,8 +411,15 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     ctx->fb = fb;
     ctx->geo = geo;
     ctx->views.assign(views, views + V);
+    ctx->frame_foveation = s->foveation;
     ctx->stream = stream;
     return FHTGS_OK;
+}
+
+// Foveation mode a view of the last frame was rendered with.
+int view_mode(fhtgs_context ctx, int view) {
+    const fhtgs_view& v = ctx->views[view];
+    return v.foveation > 0 ? v.foveation - 1 : ctx->frame_foveation;
 }
 
 fhtgs_status read_status(fhtgs_context ctx) {
@@ -597,7 +615,7 @@ fhtgs_status fhtgs_get_frame_info(fhtgs_context ctx, int32_t view, fhtgs_frame_i
     if (s.overflow & (kFrameErrSortLookback | kFrameErrStaging))
         return fail(FHTGS_ERR_CUDA, "the frame is incomplete: a bounded device wait gave up (sort look-back or attribute staging)");
     // the reference's count has a meaning only in its own foveation layout
-    out->n_instances = static_cast<int64_t>(ctx->fp.fov_mode == kFoveationReference ? s.n_instances_ref : s.n_instances);
+    out->n_instances = static_cast<int64_t>(view_mode(ctx, view) == kFoveationReference ? s.n_instances_ref : s.n_instances);
     out->instance_capacity = ctx->fp.cap;
     out->n_active_tiles = s.n_active;
     for (int k = 0; k < 6; ++k) out->partition_ranges[k] = s.ranges[k];
@@ -654,7 +672,7 @@ fhtgs_status fhtgs_copy_intermediates(fhtgs_context ctx, int32_t view, fhtgs_int
     // area tables over-count follow as sentinel keys, up to its instance count.
     // Other foveation modes have no reference layout: each stored list appears once, keyed by
     // its large tile's first sub-tile, without sentinel slots.
-    const bool ref_layout = fp.fov_mode == kFoveationReference;
+    const bool ref_layout = view_mode(ctx, view) == kFoveationReference;
     const uint64_t m_ref = ref_layout ? s.n_instances_ref : Ms;
     const uint32_t sentinel = g.end_bit <= 16 ? 0xFFFFu : 0xFFFFFFFFu;
     uint64_t pos = 0;
@@ -800,6 +818,7 @@ struct fhtgs_frame_graph_s {
     FrameBuffers fb{};
     std::vector<ViewGeom> geo;
     std::vector<fhtgs_view> views;
+    int frame_foveation = 0;
 };
 
 fhtgs_status fhtgs_frame_graph_create(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views,
@@ -862,6 +881,7 @@ fhtgs_status fhtgs_frame_graph_create(fhtgs_context ctx, const fhtgs_primitives*
     g->fb = ctx->fb;
     g->geo = ctx->geo;
     g->views = ctx->views;
+    g->frame_foveation = ctx->frame_foveation;
     *out = g;
     return FHTGS_OK;
 }
@@ -879,6 +899,7 @@ fhtgs_status fhtgs_frame_graph_launch(fhtgs_frame_graph g, void* stream_) {
     ctx->fb = g->fb;
     ctx->geo = g->geo;
     ctx->views = g->views;
+    ctx->frame_foveation = g->frame_foveation;
     ctx->stream = stream;
     ctx->launches += g->launches_per_frame;
     return FHTGS_OK;

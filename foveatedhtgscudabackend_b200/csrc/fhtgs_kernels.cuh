@@ -138,21 +138,20 @@ int launch_setup(const ViewSetup* setups, int n_views, ViewParams* out, cudaStre
 // Ring level of a large tile: squared NDC distance of the tile centre from the (clamped) gaze,
 // x and y each scaled by half the image size, in explicitly rounded IEEE steps (the CPU
 // oracle evaluates the same sequence, so both agree on every tile).
-__device__ __forceinline__ uint8_t ring_tile_type(const ViewParams& vp, const FrameParams& fp, uint32_t tx,
-                                                  uint32_t ty) {
+__device__ __forceinline__ uint8_t ring_tile_type(const ViewParams& vp, uint32_t tx, uint32_t ty) {
     const float cx = static_cast<float>(tx * kTileLarge + kTileLarge / 2);
     const float cy = static_cast<float>(ty * kTileLarge + kTileLarge / 2);
     const float dx = __fdiv_rn(__fsub_rn(cx, vp.gaze_px.x), __fmul_rn(0.5f, static_cast<float>(vp.width)));
     const float dy = __fdiv_rn(__fsub_rn(cy, vp.gaze_px.y), __fmul_rn(0.5f, static_cast<float>(vp.height)));
     const float r2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-    return r2 < fp.ring_full2 ? kFovea : r2 < fp.ring_half2 ? kPeriphery : kQuarter;
+    return r2 < vp.ring_full2 ? kFovea : r2 < vp.ring_half2 ? kPeriphery : kQuarter;
 }
 
 __device__ __forceinline__ uint8_t large_tile_type(const ViewParams& vp, const FrameParams& fp, uint32_t tile) {
     if (!tile_visible(vp.vis_mask, tile)) return kMasked;
-    if (fp.fov_mode == kFoveationNone) return kFovea;
+    if (vp.fov_mode == kFoveationNone) return kFovea;
     const uint32_t tx = tile % static_cast<uint32_t>(vp.glw), ty = tile / static_cast<uint32_t>(vp.glw);
-    if (fp.fov_mode == kFoveationRings) return ring_tile_type(vp, fp, tx, ty);
+    if (vp.fov_mode == kFoveationRings) return ring_tile_type(vp, tx, ty);
     if (in_fovea<kFoveaRadiusTiles>(tx, ty, vp.gaze_tiles))
         return in_fovea<kBlendRadiusTiles>(tx, ty, vp.gaze_tiles) ? kFovea : kBlended;
     return kPeriphery;
@@ -184,7 +183,7 @@ __global__ void __launch_bounds__(1024) classify_kernel(FrameParams fp, FrameBuf
     // partition-range kernel starts at index 1, shared_kernels.cuh:222-238); that tile is then
     // cleared instead of blended, which matches the zero-initialised output of _C.  The other
     // foveation modes have no counterpart there and no such rule.
-    const bool none = fp.fov_mode == kFoveationReference && n_active <= 1;
+    const bool none = vp.fov_mode == kFoveationReference && n_active <= 1;
     uint32_t* map = fb.tile_map_part + static_cast<size_t>(v) * fp.max_tiles;
     uint8_t* typ = fb.tile_type_part + static_cast<size_t>(v) * fp.max_tiles;
     uint8_t* lt = fb.large_type + static_cast<size_t>(v) * fp.max_large;

@@ -52,6 +52,9 @@ struct ViewParams {
     const uint32_t* fovea_sat;
     float* image;          // final image
     float* work;           // blend target of periphery/blended tiles (temp buffer when blurring)
+    int fov_mode;          // FoveationMode of this view
+    float ring_full2;      // rings: squared NDC radius of full resolution
+    float ring_half2;      // rings: squared NDC radius of 2x-down sampling (4x beyond)
 };
 
 // Host-side description of a view before the setup kernel runs.
@@ -84,9 +87,6 @@ struct FrameParams {
     int n_blocks_prim;     // preprocess/create blocks per view
     int blend_rw;          // blend: pixels per warp row (4, 8 or 16; 32 / blend_rw rows)
     int blend_blocks;      // persistent blend blocks per SM (0: as many as fit)
-    int fov_mode;          // FoveationMode
-    float ring_full2;      // rings: squared NDC radius of full resolution
-    float ring_half2;      // rings: squared NDC radius of 2x-down sampling (4x beyond)
 };
 
 // Per-view frame status written by the device, read by the host after the frame.

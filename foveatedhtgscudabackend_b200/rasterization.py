@@ -348,7 +348,7 @@ class Renderer:
                 for f in range(n.value)]
 
     def _frame(self, positions, scales, rotations, opacities, sh_0, sh_rest, settings, to_chw, blur_periphery,
-               aaa_mode, fast_math, images):
+               aaa_mode, fast_math, images, view_foveation=None):
         """C structures of one frame: (keep-alive, primitives, views array, settings, images)."""
         dev = self.device
         keep = _Keep(dev)
@@ -384,15 +384,26 @@ class Renderer:
                                  keep.u32(s.fovea_mask_area_table, "fovea_mask_area_table"), int(s.width),
                                  int(s.height), float(s.focal_x), float(s.focal_y), float(s.center_x),
                                  float(s.center_y), images[i].data_ptr())
+            if view_foveation is not None and view_foveation[i] is not None:
+                mode, *radii = view_foveation[i] if isinstance(view_foveation[i], (tuple, list)) else (view_foveation[i],)
+                if mode not in _lib.FOVEATION:
+                    raise ValueError(f"foveation must be one of {sorted(_lib.FOVEATION)}")
+                rf, rh = (list(radii) + [0.15, 0.4][len(radii):])[:2]
+                views[i].foveation = _lib.FOVEATION[mode] + 1
+                views[i].ring_full, views[i].ring_half = float(rf), float(rh)
         return keep, prims, views, st, images, n
 
     def render(self, positions, scales, rotations, opacities, sh_0, sh_rest, settings: list[RasterizerSettings],
                to_chw: bool = True, blur_periphery: bool = False, aaa_mode: bool = False, fast_math: bool = True,
-               images: list[torch.Tensor] | None = None, sync: bool = True) -> list[torch.Tensor]:
-        """Renders len(settings) views; K, SH bases, planes, scale and background of settings[0] apply."""
+               images: list[torch.Tensor] | None = None, sync: bool = True,
+               view_foveation: list | None = None) -> list[torch.Tensor]:
+        """Renders len(settings) views; K, SH bases, planes, scale and background of settings[0] apply.
+        `view_foveation[i]` (optional): view i's own foveation, "reference" / "none" or
+        ("rings", ring_full, ring_half), instead of the renderer's (set_foveation)."""
         dev = self.device
         keep, prims, views, st, images, n = self._frame(positions, scales, rotations, opacities, sh_0, sh_rest,
-                                                        settings, to_chw, blur_periphery, aaa_mode, fast_math, images)
+                                                        settings, to_chw, blur_periphery, aaa_mode, fast_math, images,
+                                                        view_foveation)
         fn = self._libh.fhtgs_render_views_sync if sync else self._libh.fhtgs_render_views
         with torch.cuda.device(dev):
             _lib.check(fn(self.ctx, C.byref(prims), views, len(settings), C.byref(st), _stream_handle(dev)))
@@ -418,10 +429,11 @@ class Renderer:
 
     def autotune(self, positions, scales, rotations, opacities, sh_0, sh_rest, settings: list[RasterizerSettings],
                  to_chw: bool = True, blur_periphery: bool = False, aaa_mode: bool = False, fast_math: bool = True,
-                 repeats: int = 5) -> dict:
+                 repeats: int = 5, view_foveation: list | None = None) -> dict:
         """Times the tuning candidates on this frame and keeps the fastest (see fhtgs_autotune)."""
         keep, prims, views, st, images, n = self._frame(positions, scales, rotations, opacities, sh_0, sh_rest,
-                                                        settings, to_chw, blur_periphery, aaa_mode, fast_math, None)
+                                                        settings, to_chw, blur_periphery, aaa_mode, fast_math, None,
+                                                        view_foveation)
         best = _lib.Tuning()
         ms = C.c_float(0.0)
         with torch.cuda.device(self.device):
@@ -436,7 +448,7 @@ class Renderer:
     def capture(self, positions, scales, rotations, opacities, sh_0, sh_rest, settings: list[RasterizerSettings],
                 to_chw: bool = True, blur_periphery: bool = False, aaa_mode: bool = False, fast_math: bool = True,
                 images: list[torch.Tensor] | None = None, gaze: torch.Tensor | None = None,
-                capacity_headroom: float = 1.25) -> "FrameGraph":
+                capacity_headroom: float = 1.25, view_foveation: list | None = None) -> "FrameGraph":
         """Captures one frame of len(settings) views into a CUDA graph (see fhtgs_frame_graph_create).
 
         All tensors are used in place by every launch: update camera matrices, masks and
@@ -444,7 +456,8 @@ class Renderer:
         tensor read at every launch (else the settings' host gaze is baked in).
         """
         keep, prims, views, st, images, n = self._frame(positions, scales, rotations, opacities, sh_0, sh_rest,
-                                                        settings, to_chw, blur_periphery, aaa_mode, fast_math, images)
+                                                        settings, to_chw, blur_periphery, aaa_mode, fast_math, images,
+                                                        view_foveation)
         gptr = None
         if gaze is not None:
             if gaze.device != self.device or gaze.dtype != torch.float32 or gaze.numel() != 2 * len(settings):

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FHTGS_ABI_VERSION 3
+#define FHTGS_ABI_VERSION 4
 
 typedef enum {
     FHTGS_OK = 0,
@@ -87,6 +87,10 @@ typedef struct {
     int32_t width, height;
     float focal_x, focal_y, center_x, center_y;
     float* image;          /* device output, [3,H,W] (to_chw) or [H,W,3]         */
+    /* per-view foveation (no counterpart in the reference): 0 = the frame's settings;
+     * 1 + fhtgs_foveation = this view's own mode, with its own ring radii */
+    int32_t foveation;
+    float ring_full, ring_half;
 } fhtgs_view;
 
 typedef struct {

@@ -8,6 +8,7 @@ median.  Also checks that the two produce identical images on the workload.
 
     python oracle/time_ref_cuda.py [--calls 100] [--n 1000000] [--width 2064 --height 2208]
     python oracle/time_ref_cuda.py --served [--duration 5 --rate 240]
+    python oracle/time_ref_cuda.py --plain
 
 --served: the served-stream trace of bench.py --workload served (3 scenes of 0.5M/2M/4M SH3
 Gaussians, seeds 1-3, stereo requests of 1440x1584 or 2064x2208 per eye), every request issued
@@ -77,6 +78,30 @@ def served(a) -> dict:
     return out
 
 
+def plain(a) -> dict:
+    """The plain single-view config (100k SH0 Gaussians, 1280x720, K = 4) through the
+    reference's `_C_benchmarking.benchmark` (its foveation cannot be switched off: centred gaze)
+    and through this package's drop-in of the same call; images compared."""
+    import torch
+
+    import foveatedhtgscudabackend_b200 as F
+    from foveatedhtgscudabackend_b200 import scene
+    import ref as REF
+
+    g = scene.make_gaussians(100_000, 0, seed=0)
+    v = scene.make_view(1280, 720)
+    gt = F.gaussians_to_torch(g)
+    st = F.settings_from_view(v, K=4, active_sh_bases=1)
+    args = (*gt, *st.as_tuple(), True, False, False)
+    ref_mod = REF.module("_C_benchmarking")
+    mine, theirs = F._C_benchmarking.benchmark(*args), ref_mod.benchmark(*args)
+    torch.cuda.synchronize()
+    return {"workload": "plain: 100k Gaussians SH0, 1280x720, K=4 (reference layout, centred gaze)",
+            "reference_cuda": timed_calls(lambda: ref_mod.benchmark(*args), a.calls),
+            "ours_dropin": timed_calls(lambda: F._C_benchmarking.benchmark(*args), a.calls),
+            "images_identical": bool(torch.equal(mine, theirs)), "gpu": torch.cuda.get_device_name()}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--calls", type=int, default=100)
@@ -85,11 +110,15 @@ def main(argv=None) -> int:
     ap.add_argument("--height", type=int, default=2208)
     ap.add_argument("--K", type=int, default=8)
     ap.add_argument("--served", action="store_true")
+    ap.add_argument("--plain", action="store_true")
     ap.add_argument("--duration", type=float, default=5.0)
     ap.add_argument("--rate", type=float, default=240.0)
     a = ap.parse_args(argv)
     if a.served:
         print(json.dumps(served(a)))
+        return 0
+    if a.plain:
+        print(json.dumps(plain(a)))
         return 0
 
     import torch

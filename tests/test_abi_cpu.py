@@ -37,7 +37,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_error_paths_without_device_work():
     lib = _lib.load()
-    assert lib.fhtgs_abi_version() == 3
+    assert lib.fhtgs_abi_version() == 4
     assert lib.fhtgs_render_views(None, None, None, 0, None, None) == 1  # invalid argument
     assert b"null" in lib.fhtgs_last_error()
     fi = _lib.FrameInfo()

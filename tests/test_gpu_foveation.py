@@ -116,3 +116,20 @@ def test_invalid_ring_settings_are_rejected(gt):
         render(gt, [v], "rings", (0.5, 0.4))
     with pytest.raises(ValueError):
         render(gt, [v], "spiral")
+
+
+def test_per_view_foveation_in_one_frame_equals_views_alone(gt):
+    """Views of one frame may carry their own foveation; each equals the view rendered alone
+    with that foveation for the whole frame."""
+    views = scene.make_batched_views(4, seed=8, radius=(3.0, 6.0), resolutions=((320, 240), (272, 400)))
+    modes = ["none", ("rings", 0.15, 100.0), ("rings", 0.15, 0.4), "reference"]
+    r = F.Renderer(DEV)
+    try:
+        st = [F.settings_from_view(v, K=8, active_sh_bases=16, device=DEV) for v in views]
+        together = [x.cpu().numpy() for x in r.render(*gt, st, fast_math=False, view_foveation=modes)]
+    finally:
+        r.close()
+    for i, (v, m) in enumerate(zip(views, modes)):
+        mode, radii = (m, (0.15, 0.4)) if isinstance(m, str) else (m[0], m[1:])
+        alone = render(gt, [v], mode, radii)[0]
+        assert np.array_equal(alone, together[i]), f"view {i} ({m})"
