@@ -70,7 +70,7 @@ def ring_samples(view, mode: str, rings) -> np.ndarray:
 def parse(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n-gaussians", type=int, default=1_000_000)
@@ -103,6 +103,11 @@ def parse(argv=None):
 # ------------------------------------------------------------------------------------------
 # clocks during the timed region
 # ------------------------------------------------------------------------------------------
+# DRAM traffic of one blend_kernel<8,8> launch of the headline frame, measured by ncu on B200
+# (385.3 MB read + 48.1 MB written; the kernel gathers ~0.95 GB of records, mostly from L2)
+BLEND_DRAM_BYTES = 433.4e6
+
+
 class ClockSampler:
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -111,13 +116,14 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.samples: list[list[str]] = []
+        self.skip = 0
         self.proc = None
         self.thread = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                          "-lms", "50", "-i", str(self.gpu)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
         except (OSError, ValueError):
             self.proc = None
@@ -128,6 +134,11 @@ class ClockSampler:
                 self.samples.append([x.strip() for x in line.split(",")])
         self.thread = threading.Thread(target=read, daemon=True)
         self.thread.start()
+        # the timed region starts once the sampler is live; samples taken before it are dropped
+        t0 = time.time()
+        while not self.samples and time.time() - t0 < 3.0 and self.proc.poll() is None:
+            time.sleep(0.005)
+        self.skip = len(self.samples)
 
     def stop(self) -> dict | None:
         if self.proc is None:
@@ -141,7 +152,8 @@ class ClockSampler:
             self.thread.join(timeout=2)
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for s in self.samples:
+        timed = self.samples[self.skip:] or self.samples
+        for s in timed:
             try:
                 sm.append(float(s[0]))
                 mx = float(s[1])
@@ -375,7 +387,11 @@ def run_ours(a, world, rank, local):
         "e2e": e2e,
         "roofline": {"bound": "fp32", "kernel": "blend_kernel<8> (all tiles of both eyes)",
                      "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
-                     "frac": round(achieved / peak_fp32, 4), "traffic": None,
+                     "frac": round(achieved / peak_fp32, 4),
+                     # DRAM bytes of one blend launch on this workload from one ncu capture
+                     # (dram__bytes_read.sum + dram__bytes_write.sum): profiles/blend_kernel_stereo_1M_2x2064x2208.md
+                     "traffic": BLEND_DRAM_BYTES if a.foveation == "reference" and a.n_gaussians == 1_000_000 else None,
+                     "traffic_unit": "bytes per launch (ncu)",
                      "peak_source": "nominal FP32 SIMT: SMs x 128 lanes x 2 x median SM clock under load",
                      "work": f"{pairs} pixel-Gaussian pairs x {FLOP_PER_PAIR} flop "
                              + ("(reference's evaluation count)" if a.foveation == "reference"
