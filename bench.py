@@ -203,17 +203,21 @@ def cpu_baseline(g, views, a, budget_s: float) -> dict:
     fov = dict(foveation=a.foveation, rings=tuple(a.rings))
     t_one, _ = O.time_views(g, [views[0]], n_threads=cores, K=a.K, active_sh_bases=(a.sh_degree + 1) ** 2,
                             precision=32, **fov)
+    stages = O.last_stage_seconds()
     sample = "one eye (left) of one stereo frame of the benchmark workload"
     total = t_one
     if 2 * t_one <= budget_s:
         t_two, _ = O.time_views(g, [views[1]], n_threads=cores, K=a.K, active_sh_bases=(a.sh_degree + 1) ** 2,
                                 precision=32, **fov)
+        stages = {k: v + w for (k, v), w in zip(stages.items(), O.last_stage_seconds().values())}
         total = t_one + t_two
         sample = "one full stereo frame (both eyes) of the benchmark workload"
     else:
         total = 2 * t_one  # second eye extrapolated from the first
+        stages = {k: 2 * v for k, v in stages.items()}
     return {"value": 1.0 / total, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": sample, "seconds": round(total, 3)}
+            "sample": sample, "seconds": round(total, 3),
+            "stage_s": {k: round(v, 3) for k, v in stages.items()}}
 
 
 # ------------------------------------------------------------------------------------------

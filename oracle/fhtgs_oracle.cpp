@@ -992,16 +992,26 @@ void preprocess_all(const oracle_scene* s, const oracle_view* v, const oracle_se
     }
 }
 
+// Wall seconds per stage (preprocess, tile classification, instance creation + sort + ranges,
+// blend + composition), summed over the views of the last oracle_time_views call.
+double g_stage_seconds[4];
+
 template <class T>
 int render_view_t(const oracle_scene* s, const oracle_view* v, const oracle_settings* st, float* image,
                   oracle_primitives* prim, oracle_tiles* tiles, oracle_instances* inst) {
+    using clk = std::chrono::steady_clock;
+    auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
     const Geometry g = geometry(v);
     std::vector<uint32_t> nt;
     std::vector<uint16_t> sb;
     std::vector<float> vpmt, rgba;
+    const auto t0 = clk::now();
     preprocess_all<T>(s, v, st, g, nt, sb, vpmt, rgba);
+    const auto t1 = clk::now();
     Tiles tl = classify(v, g);
+    const auto t2 = clk::now();
     Inst I = instances(v, g, s->n, nt.data(), sb.data());
+    const auto t3 = clk::now();
     if (image) {
         std::memset(image, 0, sizeof(float) * size_t(v->width) * v->height * 3);
         if (st->foveation == 0)
@@ -1010,6 +1020,11 @@ int render_view_t(const oracle_scene* s, const oracle_view* v, const oracle_sett
         else
             render_rings<T>(v, st, g, s->n, nt.data(), sb.data(), vpmt.data(), rgba.data(), image);
     }
+    const auto t4 = clk::now();
+    g_stage_seconds[0] += secs(t0, t1);
+    g_stage_seconds[1] += secs(t1, t2);
+    g_stage_seconds[2] += secs(t2, t3);
+    g_stage_seconds[3] += secs(t3, t4);
     if (prim) {
         if (prim->n_touched) std::memcpy(prim->n_touched, nt.data(), nt.size() * 4);
         if (prim->screen_bounds) std::memcpy(prim->screen_bounds, sb.data(), sb.size() * 2);
@@ -1106,10 +1121,15 @@ int oracle_render_view(const oracle_scene* s, const oracle_view* v, const oracle
 
 double oracle_time_views(const oracle_scene* s, const oracle_view* views, int n_views, const oracle_settings* st,
                          float* const* images) {
+    for (double& x : g_stage_seconds) x = 0.0;
     auto t0 = std::chrono::steady_clock::now();
     for (int i = 0; i < n_views; ++i) oracle_render_view(s, &views[i], st, images[i], nullptr, nullptr, nullptr);
     auto t1 = std::chrono::steady_clock::now();
     return std::chrono::duration<double>(t1 - t0).count();
+}
+
+void oracle_stage_seconds(double* out) {
+    for (int i = 0; i < 4; ++i) out[i] = g_stage_seconds[i];
 }
 
 }  // extern "C"

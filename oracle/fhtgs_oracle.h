@@ -114,6 +114,10 @@ int oracle_render_view(const oracle_scene* s, const oracle_view* v, const oracle
 /* Timing helper for the CPU baseline: renders n_views views, returns wall seconds. */
 double oracle_time_views(const oracle_scene* s, const oracle_view* views, int n_views,
                          const oracle_settings* st, float* const* images);
+/* Seconds per stage of the last oracle_time_views call (std::chrono, summed over its views):
+ * [0] preprocess, [1] tile classification, [2] instance creation + sort + ranges,
+ * [3] blend + composition. */
+void oracle_stage_seconds(double* out4);
 
 #ifdef __cplusplus
 }

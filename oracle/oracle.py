@@ -96,6 +96,8 @@ def lib():
             L.oracle_time_views.argtypes = [C.POINTER(OracleScene), C.POINTER(OracleView), C.c_int,
                                             C.POINTER(OracleSettings), C.POINTER(f32p)]
             L.oracle_time_views.restype = C.c_double
+            L.oracle_stage_seconds.argtypes = [C.POINTER(C.c_double)]
+            L.oracle_stage_seconds.restype = None
             _lib = L
     return _lib
 
@@ -293,3 +295,10 @@ def time_views(g, views, n_threads=0, **settings) -> tuple[float, list]:
     ptrs = (f32p * len(views))(*[_p(i, f32p) for i in imgs])
     secs = lib().oracle_time_views(C.byref(sc), arr, len(views), C.byref(st), ptrs)
     return float(secs), imgs
+
+
+def last_stage_seconds() -> dict:
+    """Per-stage wall seconds of the last time_views call (std::chrono inside the oracle)."""
+    out = (C.c_double * 4)()
+    lib().oracle_stage_seconds(out)
+    return dict(zip(("preprocess", "classify", "create_sort_ranges", "blend_compose"), [float(x) for x in out]))
