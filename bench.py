@@ -79,6 +79,9 @@ def parse(argv=None):
     ap.add_argument("--sh-degree", type=int, default=3)
     ap.add_argument("--K", type=int, default=8)
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--in-flight", type=int, default=2,
+                    help="stereo workload: frames in flight, one renderer context and one stream each "
+                         "(1 = one frame at a time; the single-frame numbers are reported either way)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--cpu-budget-s", type=float, default=30.0, help="upper bound of the CPU baseline sample")
@@ -267,6 +270,54 @@ def run_ours(a, world, rank, local):
     r.set_profiling(False)
     total_ms_max = max_over_ranks(total_ms, world)
     value = world * a.steps / (total_ms_max / 1000.0)
+    single = {"value": round(value, 3), "ms_per_step": round(total_ms_max / a.steps, 4),
+              "latency_ms": {"p50": round(float(np.percentile(step_ms, 50)), 4),
+                             "p99": round(float(np.percentile(step_ms, 99)), 4)}}
+
+    # ---- frames in flight: one context and one stream per frame in flight, frames issued round
+    # robin; a frame's kernels fill the SMs that the previous frame's last (densest) tiles leave
+    # idle.  Contexts are independent (own arena, own stream), so each frame is the same frame.
+    n_fl = max(1, a.in_flight)
+    rs, imgs_fl = [r], [imgs]
+    streams_fl = [stream] + [torch.cuda.Stream(dev) for _ in range(n_fl - 1)]
+    for _ in range(n_fl - 1):
+        rr = F.Renderer(dev)
+        rr.set_foveation(a.foveation, *a.rings)
+        im = [torch.empty((3, v.height, v.width), device=dev) for v in (left, right)]
+        for _ in range(1 + max(a.warmup, 0)):
+            rr.render(*gt, st, to_chw=True, fast_math=True, images=im, sync=True)
+        rs.append(rr)
+        imgs_fl.append(im)
+    if n_fl > 1:
+        launches0 = sum(x.launch_count() for x in rs)
+        clocks = ClockSampler(local)
+        clocks.start()
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fs = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+        fe = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+        e0.record(stream)
+        for sfl in streams_fl[1:]:
+            sfl.wait_event(e0)
+        for k in range(a.steps):
+            i = k % n_fl
+            with torch.cuda.stream(streams_fl[i]):
+                fs[k].record(streams_fl[i])
+                rs[i].render(*gt, st, to_chw=True, fast_math=True, images=imgs_fl[i], sync=False)
+                fe[k].record(streams_fl[i])
+        for sfl in streams_fl[1:]:
+            stream.wait_stream(sfl)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        clk = clocks.stop()
+        launches = sum(x.launch_count() for x in rs) - launches0
+        if any(x.frame_info(i)["overflow"] for x in rs for i in range(2)):
+            raise RuntimeError("instance capacity overflow inside the timed region")
+        step_ms = [fs[k].elapsed_time(fe[k]) for k in range(a.steps)]
+        total_ms_max = max_over_ranks(e0.elapsed_time(e1), world)
+        value = world * a.steps / (total_ms_max / 1000.0)
 
     # ---- dominant kernel: full-resolution blend (fovea + blended tiles), per-frame events ----
     stage_avg = {k: statistics.mean(h[k] for h in hist) for k in hist[0]}
@@ -309,30 +360,40 @@ def run_ours(a, world, rank, local):
             parts.append((i, f, t, off, nb))
             off = (off + nb + 15) // 16 * 16
     host_pack = torch.empty(off, dtype=torch.uint8, pin_memory=True)
-    dev_pack = torch.empty(off, dtype=torch.uint8, device=dev)
-    views_dev = [dict(), dict()]
     for i, f, t, o, nb in parts:
         host_pack[o:o + nb].copy_(t.reshape(-1).view(torch.uint8))
-        views_dev[i][f] = dev_pack[o:o + nb].view(t.dtype).view(t.shape)
-    sd_packed = [s._replace(**views_dev[i]) for i, s in enumerate(st)]
-    out_host = [[torch.empty((3, v.height, v.width), pin_memory=True) for v in (left, right)] for _ in range(2)]
+    # one device copy of the packed inputs per context in flight
+    dev_packs, sd_packs = [], []
+    for _ in range(n_fl):
+        dp = torch.empty(off, dtype=torch.uint8, device=dev)
+        views_dev = [dict(), dict()]
+        for i, f, t, o, nb in parts:
+            views_dev[i][f] = dp[o:o + nb].view(t.dtype).view(t.shape)
+        dev_packs.append(dp)
+        sd_packs.append([s_._replace(**views_dev[i]) for i, s_ in enumerate(st)])
+    n_buf = max(2, n_fl)
+    out_host = [[torch.empty((3, v.height, v.width), pin_memory=True) for v in (left, right)] for _ in range(n_buf)]
     h2d = int(host_pack.numel()) + 2 * 2 * 4
     d2h = sum(o.numel() * o.element_size() for o in out_host[0])
     copy_stream = torch.cuda.Stream(dev)
-    copy_done = [torch.cuda.Event(), torch.cuda.Event()]
+    copy_done = [torch.cuda.Event() for _ in range(n_buf)]
 
-    dev_imgs = [[torch.empty((3, v.height, v.width), device=dev) for v in (left, right)] for _ in range(2)]
+    dev_imgs = [[torch.empty((3, v.height, v.width), device=dev) for v in (left, right)] for _ in range(n_buf)]
 
     def e2e_step(k: int, dropin: bool):
-        cur = torch.cuda.current_stream(dev)
-        buf = k % 2
-        copy_done[buf].synchronize()  # the copy that used these buffers two steps ago has landed
-        dev_pack.copy_(host_pack, non_blocking=True)
-        sd = sd_packed
-        if dropin and a.foveation == "reference":  # the reference's call: blocking, fresh images
-            a_img, b_img = _C_stereo.render(*gt, *sd[0].as_tuple(), *sd[1].as_tuple(), True, False, False)
-        else:  # the C ABI's asynchronous frame (fhtgs_render_views) into double-buffered images
-            a_img, b_img = r.render(*gt, sd, to_chw=True, fast_math=True, images=dev_imgs[buf], sync=dropin)
+        # asynchronous path: frame k on context k % n_fl and its stream; drop-in: one context
+        buf = k % (2 if dropin else n_fl)
+        ctx = 0 if dropin else buf
+        cur = streams_fl[ctx]
+        copy_done[buf].synchronize()  # the copy that used these buffers earlier has landed
+        with torch.cuda.stream(cur):
+            dev_packs[ctx].copy_(host_pack, non_blocking=True)
+            sd = sd_packs[ctx]
+            if dropin and a.foveation == "reference":  # the reference's call: blocking, fresh images
+                a_img, b_img = _C_stereo.render(*gt, *sd[0].as_tuple(), *sd[1].as_tuple(), True, False, False)
+            else:  # the C ABI's asynchronous frame (fhtgs_render_views) into its own images
+                a_img, b_img = rs[ctx].render(*gt, sd, to_chw=True, fast_math=True, images=dev_imgs[buf],
+                                              sync=dropin)
         copy_stream.wait_stream(cur)
         with torch.cuda.stream(copy_stream):
             out_host[buf][0].copy_(a_img, non_blocking=True)
@@ -342,19 +403,21 @@ def run_ours(a, world, rank, local):
             copy_done[buf].record(copy_stream)
 
     def e2e_run(dropin: bool) -> float:
-        for k in range(2):
+        for k in range(n_buf):
             e2e_step(k, dropin)
         torch.cuda.synchronize(dev)
         barrier(world)
         t0 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
+        for sfl in streams_fl[1:]:
+            sfl.wait_event(t0)
         for k in range(e2e_steps):
             e2e_step(k, dropin)
         stream.wait_stream(copy_stream)
         t1 = torch.cuda.Event(enable_timing=True)
         t1.record(stream)
         torch.cuda.synchronize(dev)
-        if any(r.frame_info(i)["overflow"] for i in range(2)):
+        if any(x.frame_info(i)["overflow"] for x in rs for i in range(2)):
             raise RuntimeError("instance capacity overflow inside the end-to-end region")
         return max_over_ranks(t0.elapsed_time(t1), world)
 
@@ -363,9 +426,10 @@ def run_ours(a, world, rank, local):
         dropin_ms = e2e_run(dropin=True)
         e2e = {"value": round(world * e2e_steps / (e2e_ms / 1000.0), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
-               "api": "foveatedhtgscudabackend_b200.Renderer.render(sync=False) -> fhtgs_render_views (asynchronous)",
+               "api": "foveatedhtgscudabackend_b200.Renderer.render(sync=False) -> fhtgs_render_views (asynchronous), "
+                      f"{n_fl} context(s) on {n_fl} stream(s) in flight",
                "steps": e2e_steps, "h2d": "one packed copy of both eyes' inputs per step",
-               "d2h": "double-buffered pinned copies on a copy stream",
+               "d2h": f"pinned copies on a copy stream, {n_buf} buffers",
                "dropin_value": round(world * e2e_steps / (dropin_ms / 1000.0), 3),
                "dropin_api": "foveatedhtgscudabackend_b200._C_stereo.render (blocking, as the reference's call)"
                if a.foveation == "reference" else "foveatedhtgscudabackend_b200.Renderer.render(sync=True)"}
@@ -386,8 +450,11 @@ def run_ours(a, world, rank, local):
                    "views": f"2x{a.width}x{a.height}", "K": a.K, "ipd_m": 0.063,
                    "foveation": FOVEATION_TEXT[a.foveation].format(*a.rings),
                    "math": "fast (matches _C_stereo)", "l2": "inputs larger than L2 (236 MB scene, 2 x 55 MB images)",
-                   "parallelism": f"replicated scene, {world} rank(s) x 1 stereo stream"},
+                   "parallelism": f"replicated scene, {world} rank(s) x 1 stereo stream, "
+                                  f"{max(1, a.in_flight)} frame(s) in flight per rank"},
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4), "p99": round(float(np.percentile(lat, 99)), 4)},
+        "frames_in_flight": n_fl,
+        "single_frame": single,
         "e2e": e2e,
         "roofline": {"bound": "fp32", "kernel": "blend_kernel<8> (all tiles of both eyes)",
                      "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
