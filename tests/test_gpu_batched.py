@@ -169,3 +169,25 @@ def test_graph_refuses_to_run_after_the_arena_moved(batch):
     assert e.value.status == 5
     graph.close()
     r.close()
+
+
+def test_frames_in_flight_on_two_contexts_equal_one_at_a_time(batch):
+    """Two contexts on two streams with frames issued round robin (frames in flight, as the
+    benchmark runs them) render every frame exactly as one context does one frame at a time."""
+    gt, st = batch
+    alone = [x.cpu() for x in render_alone(gt, st[:2])]
+    rs = [F.Renderer(DEV), F.Renderer(DEV)]
+    streams = [torch.cuda.Stream(DEV), torch.cuda.Stream(DEV)]
+    out = [[torch.empty_like(x, device=DEV) for x in alone] for _ in range(2)]
+    try:
+        for k in range(6):
+            i = k % 2
+            with torch.cuda.stream(streams[i]):
+                rs[i].render(*gt, st[:2], images=out[i], sync=False)
+        torch.cuda.synchronize()
+        for i in range(2):
+            for a, b in zip(alone, out[i]):
+                assert torch.equal(a, b.cpu())
+    finally:
+        for r in rs:
+            r.close()
