@@ -10,9 +10,12 @@ as the reference's _C_stereo module.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints ONE JSON line (rank 0).  `value` = stereo frames/s of the whole job with the scene
-resident in HBM (device time, CUDA events, max over ranks); `e2e` = the same through the
-public drop-in call `_C_stereo.render` with the per-frame camera/gaze inputs copied from pinned
-host memory and both images copied back to the host inside the timed region; `roofline` = the
+resident in HBM and `--in-flight` frames in flight (default 2: two renderer contexts on two
+streams; device time, CUDA events, max over ranks), `single_frame` = the same one frame at a
+time; `e2e` = the same through the public C ABI's asynchronous frame with the per-frame
+camera/mask inputs copied from pinned host memory and both images copied back to the host
+inside the timed region (`dropin_value`: through the blocking drop-in `_C_stereo.render`
+instead); `roofline` = the
 dominant kernel (full-resolution K-buffer blend) measured live from per-frame CUDA events;
 `cpu_baseline` = the host-core restatement of the same algorithm (oracle) on a bounded sample.
 Multi-GPU: one process per GPU (torchrun); views are independent, so every rank renders its
