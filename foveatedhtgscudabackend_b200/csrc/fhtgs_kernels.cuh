@@ -1680,11 +1680,13 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
             const bool frag = live && !(alpha < kMinAlpha);
             float4 pm = make_float4(c.x * alpha, c.y * alpha, c.z * alpha, alpha);
             // the depth matters only to a fragment that may enter the core (alpha >= 1/20):
-            // evaluated under that test, so that warps whose fragments are all faint skip it
-            if (frag && alpha >= kMinAlphaCore) {
+            // evaluated when some lane of the warp has such a fragment (a warp-uniform branch,
+            // so that warps whose fragments are all faint skip it without reconvergence work)
+            const bool cand = frag && alpha >= kMinAlphaCore;
+            if (__any_sync(__activemask(), cand)) {
                 const float3 ep = cross(d, m) * den_rcp;
                 const float depth = dot(xyz(VPMT4), ep) + VPMT4.w;
-                if (depth < core[K - 1].depth) {
+                if (cand && depth < core[K - 1].depth) {
                     Frag f;
                     f.depth = depth;
                     f.color = pack_rgba(pm);
