@@ -110,8 +110,8 @@ def parse(argv=None):
 # clocks during the timed region
 # ------------------------------------------------------------------------------------------
 # DRAM traffic of one blend_kernel<8,8> launch of the headline frame, measured by ncu on B200
-# (385.3 MB read + 48.1 MB written; the kernel gathers ~0.95 GB of records, mostly from L2)
-BLEND_DRAM_BYTES = 433.4e6
+# (353.9 MB read + 45.3 MB written; the kernel gathers ~0.95 GB of records, mostly from L2)
+BLEND_DRAM_BYTES = 399.2e6
 
 
 class ClockSampler:
