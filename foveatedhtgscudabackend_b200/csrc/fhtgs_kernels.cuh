@@ -877,9 +877,11 @@ int launch_create(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s)
 
 // ------------------------------------------------------------------------------------------
 // stable LSD radix sort of (key, value) pairs per view (replaces cub::DeviceRadixSort::
-// SortPairs over bits [0, end_bit), inference.cu:267-274).  Digit ranking with
-// __match_any_sync per warp; counts per (digit, tile) scanned digit-major; the scatter goes
-// through shared memory so that global stores run along digit runs.
+// SortPairs over bits [0, end_bit), inference.cu:267-274).  Three-kernel form (capacities of
+// 2^30 pairs and more, and the no-allocation entry point): digit ranking with __match_any_sync
+// per warp; counts per (digit, tile) scanned digit-major; the scatter goes through shared
+// memory so that global stores run along digit runs.  Smaller capacities use the onesweep
+// pass below.
 // ------------------------------------------------------------------------------------------
 
 template <typename KeyT, int ITEMS>
@@ -1018,8 +1020,9 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_scatter_kernel(FramePara
 // Onesweep pass (one kernel per 8-bit digit, after Adinets & Merrill, "Onesweep: a faster
 // least significant digit radix sort for GPUs", 2022): a block takes the next tile of the view
 // from a ticket counter (so every earlier tile belongs to a block that already runs), ranks
-// its keys once per key with __match_any_sync (stable: warps own consecutive key runs, visited
-// in key order), publishes its digit counts, and finds the counts of all earlier tiles by
+// each key within its warp by the lanes holding the same digit (digit_peers: eight ballots;
+// stable: warps own consecutive key runs, visited in key order), publishes its digit counts,
+// and finds the counts of all earlier tiles by
 // decoupled look-back over their published words: flag kLookAggregate = this tile's own
 // count, kLookPrefix = the inclusive count of every tile up to it.  The digit's global start
 // is the exclusive sum of the pass's digit histogram (filled by the creation kernel).  The
