@@ -784,11 +784,10 @@ __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParam
         const uint64_t per_pass = ((m + tile - 1) / tile) * kSortBins;
         const uint64_t pass_stride = static_cast<uint64_t>(fb.sort_tiles) * kSortBins;
         uint32_t* look = fb.sort_look + static_cast<size_t>(v) * kSortMaxPasses * pass_stride;
-        for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * kPrimBlock + threadIdx.x; k < passes * per_pass;
-             k += static_cast<uint64_t>(gridDim.x) * kPrimBlock) {
-            const uint64_t p = k / per_pass;
-            look[p * pass_stride + (k - p * per_pass)] = 0u;
-        }
+        for (int p = 0; p < passes; ++p)
+            for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * kPrimBlock + threadIdx.x; k < per_pass;
+                 k += static_cast<uint64_t>(gridDim.x) * kPrimBlock)
+                look[p * pass_stride + k] = 0u;
     }
     __syncthreads();
     if (nv > 0) {
