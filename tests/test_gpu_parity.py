@@ -119,6 +119,11 @@ LIVE = [
     dict(module="_C_stereo", n=30000, sh_degree=3, seed=103, views=[dict(w=1032, h=1104, gaze=[500.0, 560.0], eye=-0.0315),
          dict(w=900, h=1000, gaze=[470.0, 520.0], eye=0.0315)], K=32, active_sh=16, background=2, blur=False,
          to_chw=True, aaa=False),
+    # the plain single-view config (100k SH0 Gaussians, 1280x720, K = 4, centred gaze): an
+    # instance count for which the reference's own module skips its sort, so its images are
+    # checked through the oracle while its kernels (through the harness) are compared exactly
+    dict(module="_C_benchmarking", n=100000, sh_degree=0, seed=0, views=[dict(w=1280, h=720, gaze=[640.0, 360.0])],
+         K=4, active_sh=1, background=0, blur=False, to_chw=True, aaa=False),
 ]
 
 
