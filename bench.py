@@ -271,6 +271,7 @@ def run_ours(a, world, rank, local):
         raise RuntimeError("instance capacity overflow inside the timed region")
     hist = r.stage_history(min(a.steps, 64))
     r.set_profiling(False)
+    digest = image_digest(imgs)  # the benchmark frame's images (the reference arm prints its own)
     total_ms_max = max_over_ranks(total_ms, world)
     value = world * a.steps / (total_ms_max / 1000.0)
     single = {"value": round(value, 3), "ms_per_step": round(total_ms_max / a.steps, 4),
@@ -473,6 +474,7 @@ def run_ours(a, world, rank, local):
                      "kernel_ms": round(blend_ms, 4)},
         "stage_ms": {k: round(v, 4) for k, v in stage_avg.items()},
         "instances_per_eye": [int(i["n_instances"]) for i in info],
+        "image_sha256": digest,
         "gpu_launches": int(launches),
         "clocks": clk,
     }
@@ -898,6 +900,128 @@ def run_served(a, world, rank, local):
 # ------------------------------------------------------------------------------------------
 # reference arm: the reference algorithm on the host cores
 # ------------------------------------------------------------------------------------------
+def image_digest(imgs) -> list[str]:
+    """SHA-256 of each image's float32 bytes (the same frame in both arms gives the same digest
+    exactly when the images are bit-identical)."""
+    import hashlib
+    return [hashlib.sha256(t.detach().contiguous().cpu().numpy().tobytes()).hexdigest() for t in imgs]
+
+
+def reference_cuda_leg(a, g, left, right, calls: int, warmup: int = 10) -> dict:
+    """The reference's own CUDA backend on this GPU: `_C_stereo.render` of the reference, built
+    from its sources with its own flags (+ sm_100a) into oracle/_ref, called through its pybind
+    API on the benchmark frame.  Device leg: CUDA events around each blocking call, `warmup`
+    untimed calls, then `calls` timed calls; frames/s from the median.  End-to-end leg: per call
+    the per-frame inputs of both eyes (one packed pinned host->device copy) and both images back
+    to pinned host memory, as the drop-in leg of our arm.  After the timed regions the frame is
+    rendered once by this package's drop-in and the images are compared."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref as REF  # the reference arm may load the reference build under oracle/_ref
+    import foveatedhtgscudabackend_b200 as F
+
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    try:
+        mod = REF.module("_C_stereo")
+    except ImportError as exc:
+        return {"unavailable": f"reference build not found under oracle/_ref ({exc})"}
+    dev = torch.device("cuda", torch.cuda.current_device())
+    gt = F.gaussians_to_torch(g, dev)
+    st = [F.settings_from_view(v, K=a.K, active_sh_bases=(a.sh_degree + 1) ** 2, device=dev) for v in (left, right)]
+    args = (*gt, *st[0].as_tuple(), *st[1].as_tuple(), True, False, False)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        mod.render(*args)
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    ms = []
+    for _ in range(calls):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        mod.render(*args)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
+
+    # end to end: the same per-frame copies as our drop-in leg (packed inputs in, images out)
+    fields = ("M", "VPM", "VPR_inv", "cam_position", "visibility_mask", "visibility_mask_area_table",
+              "fovea_mask_area_table")
+    parts, off = [], 0
+    for i, s_ in enumerate(st):
+        for f in fields:
+            t = getattr(s_, f).detach().cpu().contiguous()
+            t = t.view(torch.int32) if t.dtype == torch.uint32 else t
+            nb = t.numel() * t.element_size()
+            parts.append((i, f, t, off, nb))
+            off = (off + nb + 15) // 16 * 16
+    host_pack = torch.empty(off, dtype=torch.uint8, pin_memory=True)
+    for i, f, t, o, nb in parts:
+        host_pack[o:o + nb].copy_(t.reshape(-1).view(torch.uint8))
+    dev_pack = torch.empty(off, dtype=torch.uint8, device=dev)
+    views_dev = [dict(), dict()]
+    for i, f, t, o, nb in parts:
+        dt = torch.uint32 if getattr(st[i], f).dtype == torch.uint32 else t.dtype
+        views_dev[i][f] = dev_pack[o:o + nb].view(t.dtype).view(t.shape).view(dt)
+    sd = [s_._replace(**views_dev[i]) for i, s_ in enumerate(st)]
+    out_host = [[torch.empty((3, v.height, v.width), pin_memory=True) for v in (left, right)] for _ in range(2)]
+    copy_stream = torch.cuda.Stream(dev)
+    copy_done = [torch.cuda.Event() for _ in range(2)]
+
+    def e2e_step(k):
+        buf = k % 2
+        copy_done[buf].synchronize()
+        dev_pack.copy_(host_pack, non_blocking=True)
+        li, ri = mod.render(*gt, *sd[0].as_tuple(), *sd[1].as_tuple(), True, False, False)
+        copy_stream.wait_stream(stream)
+        with torch.cuda.stream(copy_stream):
+            out_host[buf][0].copy_(li, non_blocking=True)
+            out_host[buf][1].copy_(ri, non_blocking=True)
+            li.record_stream(copy_stream)
+            ri.record_stream(copy_stream)
+            copy_done[buf].record(copy_stream)
+
+    for k in range(2):
+        e2e_step(k)
+    torch.cuda.synchronize(dev)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(calls):
+        e2e_step(k)
+    stream.wait_stream(copy_stream)
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = t0.elapsed_time(t1)
+
+    theirs = mod.render(*args)
+    mine = F._C_stereo.render(*args)  # compared after the timed regions only
+    torch.cuda.synchronize(dev)
+    same = [bool(torch.equal(x, y)) for x, y in zip(mine, theirs)]
+    maxabs = [float((x - y).abs().max()) for x, y in zip(mine, theirs)]
+    psnr = [float(10 * torch.log10(1.0 / torch.clamp(((x - y).double() ** 2).mean(), min=1e-30)))
+            for x, y in zip(mine, theirs)]
+    ms_sorted = np.asarray(ms)
+    med = float(np.median(ms_sorted))
+    return {
+        "value": round(1000.0 / med, 3), "unit": UNIT,
+        "api": "oracle/_ref FoveatedHTGSCudaBackend._C_stereo.render (the reference's pybind module, built from its "
+               "sources by oracle/build_ref.sh with its own flags + sm_100a), blocking call per frame",
+        "ms": {"median": round(med, 4), "p50": round(float(np.percentile(ms_sorted, 50)), 4),
+               "p99": round(float(np.percentile(ms_sorted, 99)), 4), "mean": round(float(ms_sorted.mean()), 4)},
+        "calls": calls, "warmup_calls": warmup,
+        "e2e": {"value": round(calls / (e2e_ms / 1000.0), 3), "unit": UNIT,
+                "h2d_bytes_per_step": int(host_pack.numel()), "d2h_bytes_per_step":
+                    int(sum(o.numel() * o.element_size() for o in out_host[0])),
+                "note": "one packed pinned copy of both eyes' per-frame inputs in, both images out on a copy "
+                        "stream (2 pinned buffers), as the drop-in leg of our arm"},
+        "clocks": clk,
+        "image_sha256": image_digest(theirs),
+        "images_identical_to_ours": same, "max_abs_vs_ours": maxabs, "psnr_db_vs_ours": psnr,
+    }
+
+
 def run_reference(a, world, rank):
     if rank != 0:
         return None
@@ -906,14 +1030,21 @@ def run_reference(a, world, rank):
     # each step is the bounded sample above; K steps repeat it only when it is short
     per = 1.0 / cpu["value"]
     steps = 1 if per > 5.0 else max(1, min(a.steps, int(30.0 / max(per, 1e-3))))
+    ref_cuda = reference_cuda_leg(a, g, left, right, calls=max(100, a.steps))
     return {
         "metric": METRIC, "impl": "reference", "value": round(cpu["value"], 5), "unit": UNIT, "n_gpus": world,
         "steps": steps, "warmup": 0, "ms_per_step": round(per * 1000.0, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_gaussians": a.n_gaussians, "views": f"2x{a.width}x{a.height}", "K": a.K},
+        "config": {"workload": WORKLOAD, "n_gaussians": a.n_gaussians, "views": f"2x{a.width}x{a.height}", "K": a.K,
+                   "steps_note": f"host-core leg: {steps} step(s) of one full stereo frame each (seconds per frame on "
+                                 "the host cores), no warm-up; --steps/--warmup apply to our arm. reference_cuda leg: "
+                                 f"10 warm-up calls, then {max(100, a.steps)} timed calls",
+                   "l2": "inputs larger than L2 (236 MB scene, 2 x 55 MB images)"},
         "cpu_baseline": cpu,
         "e2e": {"value": round(cpu["value"], 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference has no CPU path; this is the host-core restatement of its algorithm (oracle/)",
+        "reference_cuda": ref_cuda,
+        "note": "value: the reference has no CPU path; this is the host-core restatement of its algorithm (oracle/). "
+                "reference_cuda: the reference's own CUDA backend on the same GPU and frame",
     }
 
 

@@ -21,6 +21,8 @@ u8p = C.POINTER(C.c_uint8)
 vp = C.c_void_p
 
 N_STAGES = 7
+WAIT_TEST_SORT_LOOKBACK = 1
+WAIT_TEST_STAGING = 2
 STAGE_NAMES = ["setup_classify", "preprocess", "scan_create", "sort", "ranges_order", "blend", "compose"]
 
 STATUS = {
@@ -133,6 +135,7 @@ SIGNATURES = {
     "fhtgs_render_views_sync": ([vp, C.POINTER(Primitives), C.POINTER(View), c_i32, C.POINTER(Settings), vp], c_i32),
     "fhtgs_get_frame_info": ([vp, c_i32, C.POINTER(FrameInfo)], c_i32),
     "fhtgs_copy_intermediates": ([vp, c_i32, C.POINTER(Intermediates)], c_i32),
+    "fhtgs_context_test_wait_timeout": ([vp, c_i32, c_i32], c_i32),
     "fhtgs_render_mono": (_MONO_ARGS, c_i32),
     "fhtgs_benchmark_mono": (_MONO_ARGS, c_i32),
     "fhtgs_render_stereo": (_STEREO_ARGS, c_i32),

@@ -2,6 +2,7 @@
 // views of a frame in the same launches, no device->host round trip inside a frame) and the
 // C ABI declared in include/fhtgs.h.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -72,6 +73,28 @@ namespace fhtgs {
 void set_last_error(const std::string& msg) { g_error = msg; }
 }  // namespace fhtgs
 
+namespace {
+// NVTX ranges of a frame in the "fhtgs" domain: one "frame" range around the enqueue and one
+// range per pipeline stage (the stages of the profiling events), so that a timeline tool shows
+// the stages and, through CUDA correlation, their kernels.  Without a tool attached each call is
+// a check of a null function pointer.
+const char* const kStageNames[FHTGS_N_STAGES] = {"setup+classify", "preprocess", "scan+create instances", "sort",
+                                                 "ranges+work order", "blend", "compose"};
+nvtxDomainHandle_t nvtx_domain() {
+    static nvtxDomainHandle_t d = nvtxDomainCreateA("fhtgs");
+    return d;
+}
+void nvtx_push(const char* name) {
+    nvtxEventAttributes_t a{};
+    a.version = NVTX_VERSION;
+    a.size = NVTX_EVENT_ATTRIB_STRUCT_SIZE;
+    a.messageType = NVTX_MESSAGE_TYPE_ASCII;
+    a.message.ascii = name;
+    nvtxDomainRangePushEx(nvtx_domain(), &a);
+}
+void nvtx_pop() { nvtxDomainRangePop(nvtx_domain()); }
+}  // namespace
+
 // Stage boundaries recorded when profiling: start | setup+classify | preprocess |
 // scan+create | sort | ranges+work order | blend | compose.
 constexpr int kStageEvents = FHTGS_N_STAGES + 1;
@@ -96,6 +119,9 @@ struct fhtgs_context_s {
     std::vector<fhtgs_view> views;
     int frame_foveation = 0;          // the settings' foveation of the last frame
     cudaStream_t stream = nullptr;
+    // armed by fhtgs_context_test_wait_timeout: the next frame's wait test and its limit
+    int wait_test = 0;
+    int wait_test_limit = 0;
     // profiling: events around the stages of the last frame, and a launch counter
     bool profile = false;
     cudaEvent_t ev[kStageRing][kStageEvents] = {};
@@ -300,6 +326,16 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     fp.n_blocks_prim = nbp;
     fp.blend_rw = ctx->tuning.blend_warp_width;
     fp.blend_blocks = ctx->tuning.blend_blocks_per_sm;
+    fp.look_spin_limit = kLookSpinLimit;
+    fp.stage_wait_limit = kStageWaitLimit;
+    fp.look_first_ticket = 0;
+    if (ctx->wait_test == FHTGS_WAIT_TEST_SORT_LOOKBACK) {
+        fp.look_spin_limit = ctx->wait_test_limit;
+        fp.look_first_ticket = 1;
+    } else if (ctx->wait_test == FHTGS_WAIT_TEST_STAGING) {
+        fp.stage_wait_limit = ctx->wait_test_limit;
+    }
+    ctx->wait_test = 0;  // one frame only
 
     FrameBuffers fb{};
     fb.views = reinterpret_cast<ViewParams*>(A + L.off_views);
@@ -377,8 +413,20 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
 
     const bool prof = ctx->profile && !ctx->capturing;
     cudaEvent_t* ev = ctx->ev[ctx->frames_profiled % kStageRing];
+    // NVTX: the frame's range and the current stage's, closed on every exit path
+    struct Ranges {
+        int open = 0;
+        Ranges() { nvtx_push("frame"); open = 1; }
+        void stage(int i) {
+            if (open > 1) { nvtx_pop(); --open; }
+            if (i < FHTGS_N_STAGES) { nvtx_push(kStageNames[i]); ++open; }
+        }
+        ~Ranges() { while (open-- > 0) nvtx_pop(); }
+    } ranges;
+    // stage boundary i: profiling event; the range of stage i - 1 ends and that of stage i starts
     auto mark = [&](int i) {
         if (prof) cudaEventRecord(ev[i], stream);
+        ranges.stage(i);
     };
     long long n = 0;
     mark(0);
@@ -567,6 +615,18 @@ fhtgs_status fhtgs_context_set_profiling(fhtgs_context ctx, int32_t enable) {
     return FHTGS_OK;
 }
 
+fhtgs_status fhtgs_context_test_wait_timeout(fhtgs_context ctx, int32_t which, int32_t limit) {
+    if (!ctx) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null context");
+    if (which != FHTGS_WAIT_TEST_SORT_LOOKBACK && which != FHTGS_WAIT_TEST_STAGING)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "which must be FHTGS_WAIT_TEST_SORT_LOOKBACK or FHTGS_WAIT_TEST_STAGING");
+    const int max_limit = which == FHTGS_WAIT_TEST_SORT_LOOKBACK ? kLookSpinLimit : kStageWaitLimit;
+    if (limit < 0 || limit > max_limit)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "limit must be in [0, " + std::to_string(max_limit) + "]");
+    ctx->wait_test = which;
+    ctx->wait_test_limit = limit;
+    return FHTGS_OK;
+}
+
 fhtgs_status fhtgs_get_stage_times(fhtgs_context ctx, float* ms, int32_t n) {
     if (!ctx || !ms || n < FHTGS_N_STAGES) return fail(FHTGS_ERR_INVALID_ARGUMENT, "need a buffer of FHTGS_N_STAGES floats");
     if (!ctx->profile || ctx->frames_profiled == 0) return fail(FHTGS_ERR_NOT_READY, "profiling off or no frame rendered");
@@ -612,8 +672,12 @@ fhtgs_status fhtgs_get_frame_info(fhtgs_context ctx, int32_t view, fhtgs_frame_i
     fhtgs_status st = read_status(ctx);
     if (st != FHTGS_OK) return st;
     const FrameStatus& s = ctx->h_status[view];
-    if (s.overflow & (kFrameErrSortLookback | kFrameErrStaging))
-        return fail(FHTGS_ERR_CUDA, "the frame is incomplete: a bounded device wait gave up (sort look-back or attribute staging)");
+    if (s.overflow & kFrameErrWait)
+        return fail(FHTGS_ERR_CUDA, std::string("the frame is incomplete: a bounded device wait gave up (") +
+                                        ((s.overflow & kFrameErrSortLookback) ? "instance sort look-back" : "") +
+                                        ((s.overflow & kFrameErrSortLookback) && (s.overflow & kFrameErrStaging) ? ", " : "") +
+                                        ((s.overflow & kFrameErrStaging) ? "preprocess attribute staging" : "") +
+                                        "); the view rendered background only");
     // the reference's count has a meaning only in its own foveation layout
     out->n_instances = static_cast<int64_t>(view_mode(ctx, view) == kFoveationReference ? s.n_instances_ref : s.n_instances);
     out->instance_capacity = ctx->fp.cap;

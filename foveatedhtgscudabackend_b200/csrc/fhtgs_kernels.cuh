@@ -548,7 +548,18 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
-constexpr int kStageWaitLimit = 1 << 20;
+// Drain after a late staging: a block must not exit while bulk copies still write into its
+// shared memory, so it waits for them, backing off, for up to kStageDrainLimit polls (seconds:
+// a copy of under 72 KB that has not landed by then means the memory system has failed, and
+// the block gives up so that the kernel still ends).
+constexpr int kStageDrainLimit = 1 << 24;
+__device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
+    for (int k = 0; k < kStageDrainLimit; ++k) {
+        if (mbar_try_wait(bar, parity)) return true;
+        __nanosleep(256);
+    }
+    return false;
+}
 
 // Bytes of one block's staged attributes (kPrimBlock Gaussians, each array 16-byte padded).
 template <typename AttrT, typename ShT>
@@ -601,12 +612,22 @@ __global__ void __launch_bounds__(kPrimBlock, 3) preprocess_kernel(FrameParams f
             bulk_g2s(d_sh0, sh_0 + 3 * static_cast<size_t>(i0), b_sh0, &s_bar);
             if (b_shr) bulk_g2s(d_shr, sh_rest + static_cast<size_t>(S3) * i0, b_shr, &s_bar);
         }
-        const bool late = __syncthreads_or(!mbar_wait_bounded(&s_bar, 0u, kStageWaitLimit));
+        const bool late = __syncthreads_or(!mbar_wait_bounded(&s_bar, 0u, fp.stage_wait_limit));
         if (late) {
-            // flag the frame, give the copies a second bounded wait, and leave this block's
-            // Gaussians unwritten (the host reports the frame as failed)
-            if (threadIdx.x == 0) for (int v = 0; v < fp.n_views; ++v) atomicOr(&fb.status[v].overflow, kFrameErrStaging);
-            __syncthreads_or(!mbar_wait_bounded(&s_bar, 0u, kStageWaitLimit));
+            // flag the frame (the host reports it as failed and the range stage skips its
+            // views), give this block's Gaussians no instances, and drain the copies still in
+            // flight before the block exits
+            const size_t N = static_cast<size_t>(fp.n_prims);
+            for (int v = 0; v < fp.n_views; ++v) {
+                const size_t o = static_cast<size_t>(v) * N + i;
+                fb.n_touched[o] = 0u;
+                fb.n_vis[o] = 0u;
+                if (threadIdx.x == 0) {
+                    fb.block_sums[static_cast<size_t>(v) * fp.n_blocks_prim + blockIdx.x] = 0u;
+                    atomicOr(&fb.status[v].overflow, kFrameErrStaging);
+                }
+            }
+            __syncthreads_or(!mbar_drain(&s_bar, 0u));
             return;
         }
         positions = reinterpret_cast<const float*>(d_pos);
@@ -710,12 +731,15 @@ __global__ void __launch_bounds__(1024) scan_blocks_kernel(FrameParams fp, Frame
     }
     if (threadIdx.x == 0) {
         fb.status[v].n_instances = static_cast<uint32_t>(carry);
-        fb.status[v].overflow = static_cast<uint32_t>(carry) > static_cast<unsigned long long>(fp.cap) ? 1u : 0u;
+        // OR: the preprocess may already have flagged a late staging in this word
+        fb.status[v].overflow |= static_cast<uint32_t>(carry) > static_cast<unsigned long long>(fp.cap) ? 1u : 0u;
     }
     if (fb.sort_ghist) {  // onesweep sort: digit counts (filled by create) and tile tickets start at 0
         for (int k = threadIdx.x; k < kSortMaxPasses * kSortBins; k += blockDim.x)
             fb.sort_ghist[static_cast<size_t>(v) * kSortMaxPasses * kSortBins + k] = 0u;
-        if (threadIdx.x < kSortMaxPasses) fb.sort_ticket[v * kSortMaxPasses + threadIdx.x] = 0u;
+        if (threadIdx.x < kSortMaxPasses)
+            fb.sort_ticket[v * kSortMaxPasses + threadIdx.x] =
+                threadIdx.x == 0 ? static_cast<uint32_t>(fp.look_first_ticket) : 0u;
     }
 }
 
@@ -883,6 +907,11 @@ int launch_create(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s)
 // pass below.
 // ------------------------------------------------------------------------------------------
 
+// Key bits that decide the order in the three-kernel form (FrameParams.sort_key_bits).
+__device__ __forceinline__ uint32_t sort_key_mask(const FrameParams& fp) {
+    return fp.sort_key_bits > 0 && fp.sort_key_bits < 32 ? (1u << fp.sort_key_bits) - 1u : 0xFFFFFFFFu;
+}
+
 template <typename KeyT, int ITEMS>
 __global__ void __launch_bounds__(kSortThreads) sort_upsweep_kernel(FrameParams fp, FrameBuffers fb, int buf, int shift) {
     constexpr int TILE = kSortThreads * ITEMS;
@@ -897,11 +926,12 @@ __global__ void __launch_bounds__(kSortThreads) sort_upsweep_kernel(FrameParams 
     const uint32_t n_here = static_cast<uint32_t>(M - t0 < static_cast<uint64_t>(TILE) ? M - t0 : TILE);
     const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[buf]) + static_cast<size_t>(v) * fp.cap + t0;
     const uint32_t wbase = static_cast<uint32_t>(warp) * 32 * ITEMS + lane;
+    const uint32_t kmask = sort_key_mask(fp);
 #pragma unroll 4
     for (int it = 0; it < ITEMS; ++it) {
         const uint32_t idx = wbase + it * 32;
         const bool ok = idx < n_here;
-        const uint32_t d = ok ? (static_cast<uint32_t>(keys[idx]) >> shift) & (kSortBins - 1) : kSortBins;
+        const uint32_t d = ok ? ((static_cast<uint32_t>(keys[idx]) & kmask) >> shift) & (kSortBins - 1) : kSortBins;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         if (ok && lane == __ffs(peers) - 1) s_hist[warp][d] += __popc(peers);
         __syncwarp();
@@ -958,6 +988,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_scatter_kernel(FramePara
     // Each warp owns 32 * ITEMS consecutive keys, visited warp-striped (coalesced loads);
     // the visit order is the key order, which makes the ranking stable.
     const uint32_t wbase = static_cast<uint32_t>(warp) * 32 * ITEMS + lane;
+    const uint32_t kmask = sort_key_mask(fp);
     KeyT k_reg[ITEMS];
     uint32_t v_reg[ITEMS];
 #pragma unroll
@@ -966,7 +997,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_scatter_kernel(FramePara
         const bool ok = idx < n_here;
         k_reg[it] = ok ? keys[idx] : static_cast<KeyT>(0);
         v_reg[it] = ok ? vals[idx] : 0u;
-        const uint32_t d = ok ? (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1) : kSortBins;
+        const uint32_t d = ok ? ((static_cast<uint32_t>(k_reg[it]) & kmask) >> shift) & (kSortBins - 1) : kSortBins;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         if (ok && lane == __ffs(peers) - 1) s_whist[warp][d] += __popc(peers);
         __syncwarp();
@@ -994,7 +1025,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_scatter_kernel(FramePara
 #pragma unroll
     for (int it = 0; it < ITEMS; ++it) {
         const bool ok = wbase + it * 32 < n_here;
-        const uint32_t dd = ok ? (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1) : kSortBins;
+        const uint32_t dd = ok ? ((static_cast<uint32_t>(k_reg[it]) & kmask) >> shift) & (kSortBins - 1) : kSortBins;
         const uint32_t peers = __match_any_sync(0xffffffffu, dd);
         const uint32_t base = ok ? s_whist[warp][dd] : 0u;
         __syncwarp();
@@ -1009,7 +1040,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_scatter_kernel(FramePara
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < n_here; j += kSortThreads) {
         const KeyT kk = s_keys[j];
-        const uint32_t dd = (static_cast<uint32_t>(kk) >> shift) & (kSortBins - 1);
+        const uint32_t dd = ((static_cast<uint32_t>(kk) & kmask) >> shift) & (kSortBins - 1);
         const uint32_t gpos = s_global_start[dd] + (j - s_local_start[dd]);
         okeys[gpos] = kk;
         ovals[gpos] = s_vals[j];
@@ -1025,11 +1056,11 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_scatter_kernel(FramePara
 // decoupled look-back over their published words: flag kLookAggregate = this tile's own
 // count, kLookPrefix = the inclusive count of every tile up to it.  The digit's global start
 // is the exclusive sum of the pass's digit histogram (filled by the creation kernel).  The
-// look-back wait is bounded: a word that stays unpublished for kLookSpinLimit reads sets
-// kFrameErrSortLookback in the frame status and the pass goes on (the host reports the error).
+// look-back wait is bounded: a word that stays unpublished for fp.look_spin_limit reads sets
+// kFrameErrSortLookback in the frame status and the pass goes on (the host reports the error
+// and the range stage skips the view).
 constexpr uint32_t kLookAggregate = 1u, kLookPrefix = 2u;
 constexpr uint32_t kLookCountMask = (1u << 30) - 1u;
-constexpr int kLookSpinLimit = 1 << 22;
 
 __device__ __forceinline__ uint32_t ld_look(const uint32_t* p) {
     uint32_t v;
@@ -1126,7 +1157,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_onesweep_kernel(FramePar
             const uint32_t w = ld_look(look + static_cast<size_t>(t) * kSortBins + d);
             const uint32_t flag = w >> 30;
             if (flag == 0u) {
-                if (++spins > kLookSpinLimit) {
+                if (++spins > fp.look_spin_limit) {
                     atomicOr(&fb.status[v].overflow, kFrameErrSortLookback);
                     s_err = 1u;
                     break;
@@ -1219,6 +1250,9 @@ int launch_sort(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s) {
 template <typename KeyT>
 __global__ void __launch_bounds__(256) ranges_kernel(FrameParams fp, FrameBuffers fb) {
     const int v = blockIdx.y;
+    // a view whose sort or staging gave up keeps empty ranges: its sorted values may come from
+    // slots that nothing wrote in this frame, and the blend must not read them
+    if (fb.status[v].overflow & kFrameErrWait) return;
     const uint64_t M = view_count(fp, fb, v);
     const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[fb.final_buf]) + static_cast<size_t>(v) * fp.cap;
     uint2* r = fb.ranges + static_cast<size_t>(v) * fp.max_large;

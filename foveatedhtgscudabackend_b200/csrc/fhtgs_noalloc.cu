@@ -11,12 +11,22 @@
 //
 // Limits and rules:
 //   * at most kNoAllocMaxPairs (1,048,576) pairs per call; larger requests are rejected;
+//   * the order is decided by the key bits below end_bit alone, as cub::DeviceRadixSort's
+//     end_bit: the last 8-bit pass masks the higher bits out of its digit, and the keys come
+//     out with all their bits;
+//   * the output buffers may be the input buffers themselves (an in-place sort); any other
+//     overlap between the four buffers is rejected;
 //   * the scratch array is shared by every call on a device and keeps the last call's
 //     contents.  Nothing in it has to start at zero: each call writes the pair count and every
 //     histogram entry it reads.  Calls that overlap on the GPU (two streams, or two host threads)
 //     race on it: serialise them;
 //   * the first call on each device looks up the array's device address (cudaGetSymbolAddress
-//     with that device current) and keeps it; make that first call before any stream capture.
+//     with that device current) and keeps it for the life of the process; make that first call
+//     before any stream capture.  A cudaDeviceReset unloads the library's device code, and the
+//     array may come back at another address, so do not reset a device while this library is in
+//     use on it;
+//   * a CUDA error left pending by an earlier call of the caller is not consumed: the sort then
+//     refuses to run and reports that error, so it is never blamed on the sort.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -60,6 +70,19 @@ fhtgs_status noalloc_fail(fhtgs_status s, const std::string& msg) {
     return s;
 }
 
+// Byte ranges [a, a + na) and [b, b + nb) share at least one byte.
+bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+    const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+    return x < y + nb && y < x + na;
+}
+
+// Error of the launch just made (launch errors are not sticky; cudaGetLastError clears them).
+fhtgs_status launch_check(const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return noalloc_fail(FHTGS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return FHTGS_OK;
+}
+
 // Device address of g_sort_scratch on the current device; looked up once per device.
 fhtgs_status scratch_for_current_device(char** out) {
     int dev = 0;
@@ -94,6 +117,18 @@ extern "C" fhtgs_status fhtgs_sort_instances_noalloc(const void* keys_in, const 
     if (n == 0) return FHTGS_OK;
     if (!keys_in || !values_in || !keys_out || !values_out)
         return noalloc_fail(FHTGS_ERR_INVALID_ARGUMENT, "null buffer");
+    const size_t kb = static_cast<size_t>(n) * key_bytes, vb = static_cast<size_t>(n) * 4;
+    const bool keys_in_place = keys_out == keys_in, values_in_place = values_out == values_in;
+    if ((!keys_in_place && overlaps(keys_out, kb, keys_in, kb)) || overlaps(keys_out, kb, values_in, vb) ||
+        (!values_in_place && overlaps(values_out, vb, values_in, vb)) || overlaps(values_out, vb, keys_in, kb) ||
+        overlaps(keys_out, kb, values_out, vb))
+        return noalloc_fail(FHTGS_ERR_INVALID_ARGUMENT,
+                            "output buffers overlap the inputs or each other (only keys_out == keys_in and "
+                            "values_out == values_in, an in-place sort, are allowed)");
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess)
+        return noalloc_fail(FHTGS_ERR_CUDA, std::string("an earlier CUDA call left an error pending (not cleared): ") +
+                                                cudaGetErrorString(e));
     char* scratch = nullptr;
     fhtgs_status st = scratch_for_current_device(&scratch);
     if (st != FHTGS_OK) return st;
@@ -103,6 +138,7 @@ extern "C" fhtgs_status fhtgs_sort_instances_noalloc(const void* keys_in, const 
     fp.n_views = 1;
     fp.key_u32 = key_bytes == 4 ? 1 : 0;
     fp.end_bit = end_bit;
+    fp.sort_key_bits = end_bit;
     fp.cap = n;
     fhtgs::FrameBuffers fb{};
     fb.status = reinterpret_cast<fhtgs::FrameStatus*>(scratch + kOffStatus);
@@ -116,17 +152,17 @@ extern "C" fhtgs_status fhtgs_sort_instances_noalloc(const void* keys_in, const 
     fb.keys[1] = scratch + kOffKeys;
     fb.vals[1] = reinterpret_cast<uint32_t*>(scratch + kOffVals);
 
-    cudaError_t e = cudaMemcpyAsync(keys_out, keys_in, static_cast<size_t>(n) * key_bytes, cudaMemcpyDeviceToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(values_out, values_in, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToDevice, s);
+    if (!keys_in_place) e = cudaMemcpyAsync(keys_out, keys_in, kb, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess && !values_in_place) e = cudaMemcpyAsync(values_out, values_in, vb, cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return noalloc_fail(FHTGS_ERR_CUDA, std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e));
     set_pair_count<<<1, 1, 0, s>>>(fb.status, static_cast<unsigned long long>(n));
+    if ((st = launch_check("pair count launch")) != FHTGS_OK) return st;
     fhtgs::kernels_fast().sort(fp, fb, s);
+    if ((st = launch_check("sort launch")) != FHTGS_OK) return st;
     if (fb.final_buf == 1) {
-        e = cudaMemcpyAsync(keys_out, fb.keys[1], static_cast<size_t>(n) * key_bytes, cudaMemcpyDeviceToDevice, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(values_out, fb.vals[1], static_cast<size_t>(n) * 4, cudaMemcpyDeviceToDevice, s);
+        e = cudaMemcpyAsync(keys_out, fb.keys[1], kb, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(values_out, fb.vals[1], vb, cudaMemcpyDeviceToDevice, s);
         if (e != cudaSuccess) return noalloc_fail(FHTGS_ERR_CUDA, std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e));
     }
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return noalloc_fail(FHTGS_ERR_CUDA, std::string("sort launch: ") + cudaGetErrorString(e));
     return FHTGS_OK;
 }

@@ -87,6 +87,16 @@ struct FrameParams {
     int n_blocks_prim;     // preprocess/create blocks per view
     int blend_rw;          // blend: pixels per warp row (4, 8 or 16; 32 / blend_rw rows)
     int blend_blocks;      // persistent blend blocks per SM (0: as many as fit)
+    int sort_key_bits;     // three-kernel sort: > 0 = only key bits below this decide the order
+                           // (higher bits are carried along, as cub's end_bit); 0 = all bits of
+                           // the sort's 8-bit passes (the renderer's keys have no higher bits)
+    // Bounded device waits (set by the host for every frame; see kLookSpinLimit and
+    // kStageWaitLimit for the defaults):
+    int look_spin_limit;   // onesweep look-back: reads of an unpublished word before giving up
+    int stage_wait_limit;  // preprocess: polls of the staging barrier before it is declared late
+                           // (0: at once, before any copy can have landed)
+    int look_first_ticket; // first ticket of the first sort pass: 0; 1 in the wait test (tile 0
+                           // is never handed out, so its look-back words are never published)
 };
 
 // Per-view frame status written by the device, read by the host after the frame.
@@ -189,5 +199,9 @@ constexpr int kSortMaxPasses = 3;     // keys of at most 24 significant bits (ti
 constexpr int64_t kOnesweepMaxCap = int64_t(1) << 30;
 constexpr uint32_t kFrameErrSortLookback = 2u;  // FrameStatus.overflow bit: look-back gave up
 constexpr uint32_t kFrameErrStaging = 4u;   // FrameStatus.overflow bit: attribute staging timed out
+constexpr uint32_t kFrameErrWait = kFrameErrSortLookback | kFrameErrStaging;
+// Default limits of the bounded device waits (FrameParams.look_spin_limit / stage_wait_limit).
+constexpr int kLookSpinLimit = 1 << 22;   // reads of an unpublished look-back word (~0.1-1 s)
+constexpr int kStageWaitLimit = 1 << 20;  // polls of the preprocess staging barrier
 
 }  // namespace fhtgs

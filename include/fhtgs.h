@@ -199,6 +199,25 @@ fhtgs_status fhtgs_render_views_sync(fhtgs_context ctx, const fhtgs_primitives* 
 fhtgs_status fhtgs_get_frame_info(fhtgs_context ctx, int32_t view, fhtgs_frame_info* out);
 fhtgs_status fhtgs_copy_intermediates(fhtgs_context ctx, int32_t view, fhtgs_intermediates* out);
 
+/* ---- tests of the bounded device-side waits ----
+ * No counterpart in the reference, whose kernels neither wait on one another nor report errors.
+ * Two stages of a frame wait on the device, each with an iteration limit after which the kernel
+ * records an error bit and returns instead of hanging: the sort's decoupled look-back over the
+ * counts that earlier tiles publish, and the preprocess's wait for the bulk copies that stage a
+ * block's Gaussians in shared memory.  A view whose wait gave up renders background only and
+ * fhtgs_get_frame_info (and the _sync calls) return FHTGS_ERR_CUDA naming the stage; the next
+ * frame is unaffected.  This call arms the NEXT frame of `ctx` (eager, or the frame a graph
+ * captures) so that one wait runs out, without any fault:
+ *   FHTGS_WAIT_TEST_SORT_LOOKBACK: tile 0 of the first sort pass is never handed out, so its
+ *     counts are never published; tile 1's look-back gives up after `limit` reads
+ *     (0 <= limit <= 4194304, the default).  Needs more than one sort tile (4096 instances).
+ *   FHTGS_WAIT_TEST_STAGING: the preprocess declares its staging late after `limit` polls
+ *     (0 <= limit <= 1048576, the default; 0 = at once), then drains the copies in flight
+ *     before the block exits.  Only the fast-math flavour stages (16-byte aligned arrays). */
+#define FHTGS_WAIT_TEST_SORT_LOOKBACK 1
+#define FHTGS_WAIT_TEST_STAGING 2
+fhtgs_status fhtgs_context_test_wait_timeout(fhtgs_context ctx, int32_t which, int32_t limit);
+
 /* ---- drop-in mirrors of the reference's positional entry points (blocking) ----
  * Arguments follow the reference's order; tensors become device pointers (+ the sizes the
  * reference reads from tensor shapes), gaze_position becomes two host floats, and the output
@@ -264,11 +283,17 @@ fhtgs_status fhtgs_render_stereo(
  * device array inside libfhtgs.so (about 8.3 MB, held by every GPU that loads the library
  * until the process exits) instead of the context arena.
  *   keys_in/values_in -> keys_out/values_out: n pairs on the current device, keys of key_bytes
- *   (2 or 4) bytes sorted stably by their low end_bit bits; inputs are not modified.
+ *   (2 or 4) bytes sorted stably by their low end_bit bits alone (higher bits are carried
+ *   along and do not affect the order, as cub's end_bit); the inputs are not modified, except
+ *   in an in-place call (keys_out == keys_in and/or values_out == values_in).  Any other
+ *   overlap between the four buffers fails with FHTGS_ERR_INVALID_ARGUMENT.
  *   n <= 1048576, larger requests fail with FHTGS_ERR_INVALID_ARGUMENT.
  * The array is shared by all calls on a device and keeps the last call's contents (nothing in
  * it needs to start at zero); calls that overlap on the GPU race on it, so serialise them.  The
- * first call on each device looks up the array's address; make it before any stream capture.
+ * first call on each device looks up the array's address and keeps it; make that call before
+ * any stream capture, and do not cudaDeviceReset a device while the library is in use on it.
+ * A CUDA error that an earlier call left pending is not consumed: the sort returns
+ * FHTGS_ERR_CUDA naming it and does not run.
  * Asynchronous on `stream`; no allocation of any kind. */
 fhtgs_status fhtgs_sort_instances_noalloc(const void* keys_in, const uint32_t* values_in,
                                           void* keys_out, uint32_t* values_out, int64_t n,

@@ -97,3 +97,18 @@ def test_server_entry_points_fail_cleanly_without_a_device():
     bad = _lib.ServerConfig(0, 9, 8, 0, 0)
     assert lib.fhtgs_server_create(C.byref(bad), C.byref(out)) == 1
     assert b"max_in_flight" in lib.fhtgs_last_error()
+
+
+def test_noalloc_sort_rejects_overlapping_buffers_before_any_device_work():
+    """Partial overlaps between the no-allocation sort's buffers are refused on the host (the
+    addresses below are never dereferenced); only exact in-place calls are allowed."""
+    lib = _lib.load()
+    n = 1000
+    base = 1 << 40
+    k_in, v_in = base, base + (1 << 20)
+    for k_out, v_out in ((k_in + 2, base + (2 << 20)),        # keys_out shifted into keys_in
+                         (base + (3 << 20), v_in + 4),        # values_out shifted into values_in
+                         (v_in, base + (3 << 20)),            # keys_out on top of values_in
+                         (base + (3 << 20), base + (3 << 20) + 8)):  # the two outputs overlap
+        assert lib.fhtgs_sort_instances_noalloc(k_in, v_in, k_out, v_out, n, 2, 13, None) == 1
+        assert b"overlap" in lib.fhtgs_last_error()

@@ -45,21 +45,21 @@ def sorted_instances_from_renderer(n, sh_degree, seed, w, h):
     return keys[order], vals[order], keys, vals, end_bit
 
 
-def noalloc_sort(keys_in: np.ndarray, vals_in: np.ndarray, end_bit: int):
+def noalloc_sort(keys_in: np.ndarray, vals_in: np.ndarray, end_bit: int, in_place: bool = False):
     lib = _lib.load()
     dev = torch.device("cuda:0")
     k_in = torch.from_numpy(keys_in).to(dev)
     v_in = torch.from_numpy(vals_in).to(dev)
-    k_out = torch.empty_like(k_in)
-    v_out = torch.empty_like(v_in)
+    k_out = k_in if in_place else torch.empty_like(k_in)
+    v_out = v_in if in_place else torch.empty_like(v_in)
     stream = torch.cuda.current_stream(dev).cuda_stream
     st = lib.fhtgs_sort_instances_noalloc(k_in.data_ptr(), v_in.data_ptr(), k_out.data_ptr(), v_out.data_ptr(),
                                           int(keys_in.size), int(keys_in.itemsize), int(end_bit), stream)
     _lib.check(st)
     torch.cuda.synchronize(dev)
     out = (k_out.cpu().numpy(), v_out.cpu().numpy())
-    # the inputs are left as they were
-    assert np.array_equal(k_in.cpu().numpy(), keys_in) and np.array_equal(v_in.cpu().numpy(), vals_in)
+    if not in_place:  # the inputs are left as they were
+        assert np.array_equal(k_in.cpu().numpy(), keys_in) and np.array_equal(v_in.cpu().numpy(), vals_in)
     return out
 
 
@@ -79,3 +79,25 @@ def test_noalloc_sort_rejects_sizes_beyond_its_maximum():
     st = lib.fhtgs_sort_instances_noalloc(None, None, None, None, MAX_PAIRS + 1, 4, 17, None)
     assert st == 1
     assert b"1048576" in lib.fhtgs_last_error()
+
+
+def test_noalloc_sort_orders_by_the_bits_below_end_bit_only():
+    """Keys with bits set at and above end_bit (end_bit not a multiple of 8): the order is the
+    stable order of the low end_bit bits, and every key comes out with all its bits."""
+    rng = np.random.default_rng(7)
+    for dtype, end_bit, n in ((np.uint16, 11, 70_000), (np.uint32, 17, 300_001), (np.uint32, 20, 4097)):
+        keys = rng.integers(0, np.iinfo(dtype).max, size=n, dtype=np.uint64).astype(dtype)
+        vals = rng.permutation(n).astype(np.uint32)
+        order = np.argsort(keys.astype(np.uint64) & ((1 << end_bit) - 1), kind="stable")
+        got_k, got_v = noalloc_sort(keys, vals, end_bit)
+        assert np.array_equal(got_k, keys[order]), f"{dtype.__name__} end_bit {end_bit}"
+        assert np.array_equal(got_v, vals[order]), f"{dtype.__name__} end_bit {end_bit}"
+
+
+def test_noalloc_sort_in_place_equals_out_of_place():
+    rng = np.random.default_rng(3)
+    keys = rng.integers(0, 1 << 13, size=200_000, dtype=np.uint16)
+    vals = np.arange(keys.size, dtype=np.uint32)
+    ref = noalloc_sort(keys, vals, 13)
+    got = noalloc_sort(keys, vals, 13, in_place=True)
+    assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
