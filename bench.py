@@ -1050,7 +1050,14 @@ def run_reference(a, world, rank):
 
 def main(argv=None) -> int:
     a = parse(argv)
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # not under a launcher: start the --gpus ranks here (one process per GPU, torchrun on
+        # 127.0.0.1); each rank runs this script with the same arguments
+        from foveatedhtgscudabackend_b200 import dist as D
+        return D.launch_ranks(a.gpus, [os.path.abspath(__file__)] + list(sys.argv[1:] if argv is None else argv))
     world, rank, local = dist_setup(a)
+    if world != a.gpus:
+        raise SystemExit(f"bench.py: --gpus {a.gpus} but {world} rank(s) were started")
     try:
         if a.impl == "reference":
             line = run_reference(a, world, rank)
