@@ -17,10 +17,10 @@ from .rasterization import (  # noqa: F401
     _C_stereo,
 )
 from ._lib import FhtgsError  # noqa: F401
-from .serving import Completion, Server  # noqa: F401
+from .serving import Completion, Server, ServerGroup  # noqa: F401
 from .display import FoveatedHTGSVisualizer, _C_visualization, build_tile_masks, pack_display  # noqa: F401
 from .torch_scene import from_half_storage, gaussians_to_torch, settings_from_view, to_half_storage  # noqa: F401
 
 __all__ = ["FoveatedHTGSRasterizer", "FoveatedHTGSVisualizer", "RasterizerSettings", "BackgroundModel",
            "GazeVisualizationType", "Renderer", "FhtgsError", "gaussians_to_torch", "settings_from_view",
-           "build_tile_masks", "pack_display", "Server", "Completion"]
+           "build_tile_masks", "pack_display", "Server", "ServerGroup", "Completion"]

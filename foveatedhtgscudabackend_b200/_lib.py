@@ -106,6 +106,10 @@ class Completion(C.Structure):
                 ("images", vp * 2), ("message", C.c_char * 96)]
 
 
+class GroupCompletion(C.Structure):
+    _fields_ = [("completion", Completion), ("replica", c_i32), ("device", c_i32)]
+
+
 class ServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("submitted", "completed", "failed", "frames", "views", "retries", "queued",
                                          "in_flight", "resident_bytes", "peak_resident_bytes", "admission_waits",
@@ -159,6 +163,16 @@ SIGNATURES = {
     "fhtgs_server_drain": ([vp, c_i32], c_i32),
     "fhtgs_server_get_stats": ([vp, C.POINTER(ServerStats)], c_i32),
     "fhtgs_server_clock_ms": ([vp], C.c_double),
+    "fhtgs_server_group_create": ([C.POINTER(c_i32), c_i32, C.POINTER(ServerConfig), C.POINTER(vp)], c_i32),
+    "fhtgs_server_group_destroy": ([vp], c_i32),
+    "fhtgs_server_group_size": ([vp], c_i32),
+    "fhtgs_server_group_add_scene": ([vp, c_i32, C.POINTER(Primitives), C.POINTER(Settings), C.POINTER(c_i32)], c_i32),
+    "fhtgs_server_group_remove_scene": ([vp, c_i32], c_i32),
+    "fhtgs_server_group_submit": ([vp, C.POINTER(Request), C.POINTER(C.c_int64), C.POINTER(c_i32)], c_i32),
+    "fhtgs_server_group_poll": ([vp, C.POINTER(GroupCompletion), c_i32, c_i32, C.POINTER(c_i32)], c_i32),
+    "fhtgs_server_group_release": ([vp, C.c_int64], c_i32),
+    "fhtgs_server_group_drain": ([vp, c_i32], c_i32),
+    "fhtgs_server_group_get_stats": ([vp, c_i32, C.POINTER(ServerStats), C.POINTER(C.c_int64)], c_i32),
     "fhtgs_build_tile_masks": ([vp, c_i32, c_i32, vp, vp, vp, vp], c_i32),
     "fhtgs_pack_display": ([C.POINTER(vp), c_i32, c_i32, c_i32, c_i32, c_i32, vp, vp], c_i32),
     "fhtgs_visualize_gaze": ([vp, c_i32, c_i32, c_f, c_f, c_f, c_f, c_f, c_i32, c_i32, c_i32, vp], c_i32),

@@ -9,6 +9,7 @@ Translation units:
   csrc/fhtgs_noalloc.cu the instance sort with a static working array
   csrc/fhtgs_extras.cu  tile-mask builder, display packing, debug overlays
   csrc/fhtgs_server.cu  request server: resident scenes, continuous batching, HBM admission
+  csrc/fhtgs_group.cu   replica group of servers over several devices (routing: fhtgs_route.h)
 The CUDA runtime is linked statically; the library has no torch dependency.
 """
 from __future__ import annotations
@@ -37,8 +38,9 @@ UNITS = [
     ("fhtgs_noalloc.cu", []),
     ("fhtgs_extras.cu", []),
     ("fhtgs_server.cu", []),
+    ("fhtgs_group.cu", []),
 ]
-HEADERS = ["fhtgs_types.cuh", "fhtgs_math.cuh", "fhtgs_kernels.cuh", "fhtgs_internal.h"]
+HEADERS = ["fhtgs_types.cuh", "fhtgs_math.cuh", "fhtgs_kernels.cuh", "fhtgs_internal.h", "fhtgs_route.h"]
 
 
 def nvcc() -> str:

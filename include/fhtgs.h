@@ -463,6 +463,52 @@ fhtgs_status fhtgs_server_drain(fhtgs_server server, int32_t timeout_ms);
 fhtgs_status fhtgs_server_get_stats(fhtgs_server server, fhtgs_server_stats* out);
 double fhtgs_server_clock_ms(fhtgs_server server);   /* ms since the server was created */
 
+/* ---- several GPUs: a replica group of servers ----
+ * No counterpart in the reference (one GPU; one view or stereo pair per blocking call).
+ * Views are independent once their camera is known, and the K-buffer blend cannot merge partial
+ * results over a split of the Gaussians (the core is quantised to RGBA8 as fragments arrive), so
+ * several GPUs serve more requests by each holding a REPLICA of every scene and rendering each
+ * request, whole, on one of them.  A group owns one server per entry of `devices` (configured by
+ * `config`, whose device field is ignored); a device may appear more than once (several
+ * replicas on one GPU).  Nothing crosses devices per frame: no collective, no peer traffic.
+ *  - add_scene: the caller's arrays (and background data) lie on `home_device`.  The first
+ *    replica on that device borrows them; every other replica gets its own copy in its device's
+ *    HBM (cudaMemcpyPeerAsync; the call returns once the copies landed), counted in its server's
+ *    budget.  Copies are freed when the group is destroyed.
+ *  - submit: the request goes, whole, to the replica with the least outstanding work: the
+ *    pixels of its eyes times (1 + Gaussians / 262144), summed over the requests routed to it
+ *    whose completions have not been polled yet; ties go round robin.  A request whose eyes carry
+ *    device buffers (masks, tables, output images) is routed among the replicas on the device of
+ *    those buffers; one without any goes to any replica and gets server-owned outputs there.
+ *    `replica` (may be NULL) receives the replica's index.
+ *  - poll: completions of every replica, in group tickets, with the replica and its device.
+ *  - get_stats: one replica's server statistics and its outstanding work. */
+typedef struct fhtgs_server_group_s* fhtgs_server_group;
+
+typedef struct {
+    fhtgs_completion completion;   /* ticket: the group's ticket                                  */
+    int32_t replica;               /* index into the group's devices                              */
+    int32_t device;                /* where completion.images lie                                 */
+} fhtgs_group_completion;
+
+fhtgs_status fhtgs_server_group_create(const int32_t* devices, int32_t n_devices,
+                                       const fhtgs_server_config* config, fhtgs_server_group* out);
+/* Destroys every replica's server (running frames finish) and frees the scene copies. */
+fhtgs_status fhtgs_server_group_destroy(fhtgs_server_group group);
+int32_t fhtgs_server_group_size(fhtgs_server_group group);
+fhtgs_status fhtgs_server_group_add_scene(fhtgs_server_group group, int32_t home_device,
+                                          const fhtgs_primitives* prims, const fhtgs_settings* settings,
+                                          int32_t* scene_id);
+fhtgs_status fhtgs_server_group_remove_scene(fhtgs_server_group group, int32_t scene_id);
+fhtgs_status fhtgs_server_group_submit(fhtgs_server_group group, const fhtgs_request* request,
+                                       int64_t* ticket, int32_t* replica);
+fhtgs_status fhtgs_server_group_poll(fhtgs_server_group group, fhtgs_group_completion* out,
+                                     int32_t max_completions, int32_t wait_ms, int32_t* n_out);
+fhtgs_status fhtgs_server_group_release(fhtgs_server_group group, int64_t ticket);
+fhtgs_status fhtgs_server_group_drain(fhtgs_server_group group, int32_t timeout_ms);
+fhtgs_status fhtgs_server_group_get_stats(fhtgs_server_group group, int32_t replica, fhtgs_server_stats* out,
+                                          int64_t* outstanding_cost);
+
 /* ---- tile masks on the device ----
  * No counterpart in the reference, which takes the three mask tensors precomputed by the
  * calling framework (torch_bindings/rasterization.py:22-43; read at

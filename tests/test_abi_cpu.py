@@ -61,7 +61,7 @@ def test_struct_layouts_match_the_header(tmp_path):
                "fhtgs_frame_info": _lib.FrameInfo, "fhtgs_intermediates": _lib.Intermediates,
                "fhtgs_tuning": _lib.Tuning, "fhtgs_server_config": _lib.ServerConfig, "fhtgs_eye": _lib.Eye,
                "fhtgs_request": _lib.Request, "fhtgs_completion": _lib.Completion,
-               "fhtgs_server_stats": _lib.ServerStats}
+               "fhtgs_server_stats": _lib.ServerStats, "fhtgs_group_completion": _lib.GroupCompletion}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for cname, py in structs.items():
         ctype = "struct fhtgs_tuning" if cname == "fhtgs_tuning" else cname
@@ -112,3 +112,16 @@ def test_noalloc_sort_rejects_overlapping_buffers_before_any_device_work():
                          (base + (3 << 20), base + (3 << 20) + 8)):  # the two outputs overlap
         assert lib.fhtgs_sort_instances_noalloc(k_in, v_in, k_out, v_out, n, 2, 13, None) == 1
         assert b"overlap" in lib.fhtgs_last_error()
+
+
+def test_server_group_entry_points_fail_cleanly_without_a_device():
+    lib = _lib.load()
+    cfg = _lib.ServerConfig(0, 2, 8, 0, 0)
+    out = _lib.vp()
+    devs = (C.c_int32 * 2)(0, 0)
+    assert lib.fhtgs_server_group_create(devs, 0, C.byref(cfg), C.byref(out)) == 1
+    assert lib.fhtgs_server_group_create(devs, 2, C.byref(cfg), C.byref(out)) != 0  # no CUDA device here
+    assert not out.value
+    assert lib.fhtgs_server_group_size(None) == 0
+    assert lib.fhtgs_server_group_destroy(None) == 0
+    assert lib.fhtgs_server_group_submit(None, None, None, None) == 1
