@@ -47,10 +47,11 @@ def arm(r, which, limit):
     _lib.check(r._libh.fhtgs_context_test_wait_timeout(r.ctx, which, limit))
 
 
+# The staging wait is tested with a limit of 0 polls (it gives up before it looks): a single
+# mbarrier poll may suspend the thread until the copies land, so any larger limit may not run out.
 @pytest.mark.parametrize("which,limit,stage", [
     (_lib.WAIT_TEST_SORT_LOOKBACK, 10_000, "look-back"),
     (_lib.WAIT_TEST_STAGING, 0, "staging"),
-    (_lib.WAIT_TEST_STAGING, 1, "staging"),
 ])
 def test_wait_runs_out_is_reported_and_the_next_frame_is_exact(frame, which, limit, stage):
     r = F.Renderer("cuda:0")
