@@ -96,6 +96,10 @@ def parse(argv=None):
     ap.add_argument("--n-views", type=int, default=64, help="cameras per batch (batched workload)")
     ap.add_argument("--duration", type=float, default=10.0, help="seconds of arrivals (served workload)")
     ap.add_argument("--rate", type=float, default=240.0, help="request arrivals per second (served workload)")
+    ap.add_argument("--rate-sweep", type=float, nargs="*", default=[40.0, 60.0, 80.0, 100.0, 120.0],
+                    help="served workload: further Poisson rates (requests/s) replayed for --sweep-duration s each; "
+                         "p50/p99 and achieved requests/s per rate (empty: none)")
+    ap.add_argument("--sweep-duration", type=float, default=6.0)
     ap.add_argument("--slots", type=int, default=2, help="frames in flight (served workload)")
     ap.add_argument("--max-batch", type=int, default=8, help="requests per frame (served workload)")
     ap.add_argument("--no-plain", action="store_true", help="served workload: skip the plain per-request path")
@@ -788,32 +792,39 @@ def run_served(a, world, rank, local):
         srv.resume()
         drain_all(len(warm))
 
+    def replay(tr, prep):
+        """Poisson replay of a trace through the server: latency (GPU completion - scheduled
+        arrival) per request, seconds from the first arrival to the last completion, and the
+        views of the frame that rendered each request."""
+        n = len(tr)
+        t0 = srv.clock_ms() + 20.0
+        arrive = [t0 + 1000.0 * t for t, *_ in tr]
+        lat = [0.0] * n
+        fviews = []
+        i = done = 0
+        last = t0
+        while done < n:
+            now = srv.clock_ms()
+            while i < n and arrive[i] <= now:
+                srv.submit_prepared(prep[i])
+                i += 1
+            wait = int(min(max(arrive[i] - srv.clock_ms() - 1.0, 0.0), 5.0)) if i < n else 5
+            for c in srv.poll(max_completions=256, wait_ms=wait):
+                if not c.ok:
+                    raise RuntimeError(f"request failed: {c.message}")
+                lat[c.tag] = c.done_ms - arrive[c.tag]
+                last = max(last, c.done_ms)
+                fviews.append(c.frame_views)
+                srv.release(c.ticket)
+                done += 1
+        return lat, (last - t0) / 1000.0, fviews
+
     prepared = [srv.prepare(ids[si], [l, r], tag=k) for k, (t, si, l, r) in enumerate(trace)]
     stats0 = srv.stats()
     clocks = ClockSampler(local)
     clocks.start()
     # (a) server, Poisson replay
-    t0 = srv.clock_ms() + 20.0
-    arrive = [t0 + 1000.0 * t for t, *_ in trace]
-    lat_s = [0.0] * n_req
-    frame_views = []
-    i = done = 0
-    last_done = t0
-    while done < n_req:
-        now = srv.clock_ms()
-        while i < n_req and arrive[i] <= now:
-            srv.submit_prepared(prepared[i])
-            i += 1
-        wait = int(min(max(arrive[i] - srv.clock_ms() - 1.0, 0.0), 5.0)) if i < n_req else 5
-        for c in srv.poll(max_completions=256, wait_ms=wait):
-            if not c.ok:
-                raise RuntimeError(f"request failed: {c.message}")
-            lat_s[c.tag] = c.done_ms - arrive[c.tag]
-            last_done = max(last_done, c.done_ms)
-            frame_views.append(c.frame_views)
-            srv.release(c.ticket)
-            done += 1
-    served_s = (last_done - t0) / 1000.0
+    lat_s, served_s, frame_views = replay(trace, prepared)
     stats1 = srv.stats()
     # saturated: the whole trace at once
     srv.pause()
@@ -830,10 +841,28 @@ def run_served(a, world, rank, local):
             got += 1
     served_sat = n_req / ((sat_done - ts) / 1000.0)
     clk = clocks.stop()
+    # rate sweep: the same server at further Poisson rates (each its own seeded trace)
+    pct = lambda x, q: round(float(np.percentile(x, q)), 3)
+    sweep = []
+    for rate in a.rate_sweep:
+        tr = scene.make_served_requests(a.sweep_duration, rate, len(scenes), seed=2000 + int(rate) + rank)
+        prep = [srv.prepare(ids[si], [l, r], tag=k) for k, (t, si, l, r) in enumerate(tr)]
+        lat, secs, fv = replay(tr, prep)
+        by_scene = {}
+        for k, (t, si, l, r) in enumerate(tr):
+            by_scene.setdefault(SERVED_SCENES[si], []).append(lat[k])
+        achieved = len(tr) / secs
+        offered = len(tr) / max(tr[-1][0], 1e-9) if tr else 0.0  # this trace's own arrival rate
+        sweep.append({"rate_per_s": rate, "requests": len(tr), "offered_per_s": round(offered, 2),
+                      "achieved_per_s": round(achieved, 2),
+                      # keeps up: completions follow the arrivals (within 5 %) and the last
+                      # request did not wait a whole second longer than the median one
+                      "keeps_up": bool(achieved >= 0.95 * offered and max(lat) < np.median(lat) + 1000.0), "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+                      "p99_ms_by_scene": {str(n): pct(x, 99) for n, x in sorted(by_scene.items())},
+                      "mean_frame_views": round(float(np.mean(fv)), 2)})
     srv.close()
 
     # (b) plain per-request path on the same trace (device settings prepared beforehand)
-    pct = lambda x, q: round(float(np.percentile(x, q)), 3)
     plain = None
     if not a.no_plain:
         if a.foveation == "reference":
@@ -891,6 +920,8 @@ def run_served(a, world, rank, local):
         "throughput_vs_plain": round((n_req / served_s) / plain["requests_per_s"], 3) if plain else None,
         "saturated_vs_plain": round(served_sat / plain["saturated_requests_per_s"], 3) if plain else None,
         "mean_frame_views": round(float(np.mean(frame_views)), 2),
+        "rate_sweep": sweep,
+        "highest_sustained_rate_per_s": max([x["rate_per_s"] for x in sweep if x["keeps_up"]], default=None),
         "server": {k: stats1[k] - stats0.get(k, 0) if k in ("frames", "views", "retries", "admission_waits") else stats1[k]
                    for k in ("frames", "views", "retries", "admission_waits", "peak_resident_bytes", "max_frame_requests")},
         "clocks": clk,
