@@ -773,10 +773,12 @@ def run_served(a, world, rank, local):
 
     def drain_all(expect):
         got = 0
+        idle = 0
         while got < expect:
             cs = srv.poll(max_completions=256, wait_ms=1000)
-            if not cs:
-                raise RuntimeError("server made no progress")
+            idle = 0 if cs else idle + 1
+            if idle >= 60:  # frames of many large views take seconds; a minute without any is a fault
+                raise RuntimeError("server made no progress for 60 s")
             for c in cs:
                 if not c.ok:
                     raise RuntimeError(f"request failed: {c.message}")

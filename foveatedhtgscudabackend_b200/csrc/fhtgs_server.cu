@@ -547,12 +547,24 @@ void worker_main(fhtgs_server_s* S) {
     cudaSetDevice(S->cfg.device);
     std::unique_lock<std::mutex> lk(S->mu);
     for (;;) {
+        // Stopping, the thread waits (with `mu` released) for the running frames' completion
+        // callbacks, which take `mu`, and leaves once no frame runs: a predicate that held while
+        // frames still ran would keep `mu` locked and the callbacks out for good.
         S->cv.wait(lk, [&] {
-            return S->stop || any_done_locked(S) ||
-                   (!S->paused && !S->queue.empty() && !S->mem_blocked && free_slot_locked(S) >= 0);
+            return any_done_locked(S) || (S->stop && !any_busy_locked(S)) ||
+                   (!S->stop && !S->paused && !S->queue.empty() && !S->mem_blocked && free_slot_locked(S) >= 0);
         });
         reap_locked(S);
-        if (S->stop && S->queue.empty() && !any_busy_locked(S)) break;
+        if (S->stop) {
+            // shutting down: requests queued again by the reaping (an instance overflow) fail
+            // like the rest of the queue; no new frame is launched
+            while (!S->queue.empty()) {
+                complete_locked(S, S->queue.front(), FHTGS_ERR_NOT_READY, 0, ms_since(S->t0), "server shut down");
+                S->queue.pop_front();
+            }
+            if (!any_busy_locked(S)) break;
+            continue;
+        }
         if (!S->paused) schedule_locked(S, lk);
     }
     S->cv_done.notify_all();

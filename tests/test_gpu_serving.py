@@ -295,3 +295,25 @@ def test_ring_foveation_scenes_match_the_renderer(scenes):
         for c in comps:
             for e in range(2):
                 assert torch.equal(c.images[e], ref[c.tag][e]), f"request {c.tag} eye {e}"
+
+
+def test_destroy_with_frames_in_flight_returns(scenes):
+    """Closing a server while its frames run: the running frames finish, queued requests are
+    dropped, and the call returns (the scheduler waits for the frames' completion callbacks with
+    its lock released; it once spun holding the lock those callbacks need)."""
+    import threading
+    import time
+
+    reqs = make_requests(16, len(scenes), seed=21)
+    srv = Server(DEV, max_in_flight=2, max_batch_requests=2)
+    ids = add_all(srv, scenes)
+    for k, (si, eyes) in enumerate(reqs):
+        srv.submit(ids[si], eyes, tag=k)
+    time.sleep(0.005)  # the first frames are on the GPU, the rest queued
+    t = threading.Thread(target=srv.close, daemon=True)
+    t0 = time.perf_counter()
+    t.start()
+    t.join(30.0)
+    assert not t.is_alive(), "fhtgs_server_destroy did not return within 30 s"
+    assert time.perf_counter() - t0 < 30.0
+    torch.cuda.synchronize()
