@@ -821,6 +821,25 @@ def run_served(a, world, rank, local):
                 done += 1
         return lat, (last - t0) / 1000.0, fviews
 
+    # latency floor: each scene and resolution served alone, one request at a time (median of 5)
+    alone = {}
+    for si in range(len(scenes)):
+        for (t, si_, l, r) in warm:
+            key = f"{SERVED_SCENES[si]}@{l.width}x{l.height}"
+            if key in alone:
+                continue
+            lat1 = []
+            for _ in range(5):
+                tk = srv.submit(ids[si], [l, r])
+                c = []
+                while not c:
+                    c = srv.poll(max_completions=1, wait_ms=1000)
+                lat1.append(c[0].done_ms - c[0].submit_ms)
+                srv.release(c[0].ticket)
+            alone[key] = round(float(np.median(lat1)), 3)
+            if len(alone) == 2 * (si + 1):
+                break
+
     prepared = [srv.prepare(ids[si], [l, r], tag=k) for k, (t, si, l, r) in enumerate(trace)]
     stats0 = srv.stats()
     clocks = ClockSampler(local)
@@ -922,6 +941,7 @@ def run_served(a, world, rank, local):
         "throughput_vs_plain": round((n_req / served_s) / plain["requests_per_s"], 3) if plain else None,
         "saturated_vs_plain": round(served_sat / plain["saturated_requests_per_s"], 3) if plain else None,
         "mean_frame_views": round(float(np.mean(frame_views)), 2),
+        "alone_latency_ms": alone,
         "rate_sweep": sweep,
         "highest_sustained_rate_per_s": max([x["rate_per_s"] for x in sweep if x["keeps_up"]], default=None),
         "server": {k: stats1[k] - stats0.get(k, 0) if k in ("frames", "views", "retries", "admission_waits") else stats1[k]
