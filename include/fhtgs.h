@@ -206,8 +206,8 @@ fhtgs_status fhtgs_copy_intermediates(fhtgs_context ctx, int32_t view, fhtgs_int
  * counts that earlier tiles publish, and the preprocess's wait for the bulk copies that stage a
  * block's Gaussians in shared memory.  A view whose wait gave up renders background only and
  * fhtgs_get_frame_info (and the _sync calls) return FHTGS_ERR_CUDA naming the stage; the next
- * frame is unaffected.  This call arms the NEXT frame of `ctx` (eager, or the frame a graph
- * captures) so that one wait runs out, without any fault:
+ * frame is unaffected.  This call arms the next frame `ctx` renders (fhtgs_frame_graph_create
+ * renders one eagerly first, which consumes it) so that one wait runs out, without any fault:
  *   FHTGS_WAIT_TEST_SORT_LOOKBACK: tile 0 of the first sort pass is never handed out, so its
  *     counts are never published; tile 1's look-back gives up after `limit` reads
  *     (0 <= limit <= 4194304, the default).  Needs more than one sort tile (4096 instances).
