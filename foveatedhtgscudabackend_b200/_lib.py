@@ -23,7 +23,7 @@ vp = C.c_void_p
 N_STAGES = 7
 WAIT_TEST_SORT_LOOKBACK = 1
 WAIT_TEST_STAGING = 2
-STAGE_NAMES = ["setup_classify", "preprocess", "scan_create", "sort", "ranges_order", "blend", "compose"]
+STAGE_NAMES = ["setup", "preprocess_classify", "scan_create", "sort", "ranges_order", "blend", "compose"]
 
 STATUS = {
     0: "FHTGS_OK",

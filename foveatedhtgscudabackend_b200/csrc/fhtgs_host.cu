@@ -78,7 +78,7 @@ namespace {
 // range per pipeline stage (the stages of the profiling events), so that a timeline tool shows
 // the stages and, through CUDA correlation, their kernels.  Without a tool attached each call is
 // a check of a null function pointer.
-const char* const kStageNames[FHTGS_N_STAGES] = {"setup+classify", "preprocess", "scan+create instances", "sort",
+const char* const kStageNames[FHTGS_N_STAGES] = {"setup", "preprocess+classify", "scan+create instances", "sort",
                                                  "ranges+work order", "blend", "compose"};
 nvtxDomainHandle_t nvtx_domain() {
     static nvtxDomainHandle_t d = nvtxDomainCreateA("fhtgs");
@@ -95,7 +95,7 @@ void nvtx_push(const char* name) {
 void nvtx_pop() { nvtxDomainRangePop(nvtx_domain()); }
 }  // namespace
 
-// Stage boundaries recorded when profiling: start | setup+classify | preprocess |
+// Stage boundaries recorded when profiling: start | setup | preprocess (classification beside it) |
 // scan+create | sort | ranges+work order | blend | compose.
 constexpr int kStageEvents = FHTGS_N_STAGES + 1;
 constexpr int kStageRing = 64;   // frames whose stage events are kept
@@ -119,6 +119,10 @@ struct fhtgs_context_s {
     std::vector<fhtgs_view> views;
     int frame_foveation = 0;          // the settings' foveation of the last frame
     cudaStream_t stream = nullptr;
+    // tile classification runs on a second stream beside the preprocess (forked and joined
+    // with these events inside every frame)
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     // armed by fhtgs_context_test_wait_timeout: the next frame's wait test and its limit
     int wait_test = 0;
     int wait_test_limit = 0;
@@ -431,9 +435,17 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     long long n = 0;
     mark(0);
     FHTGS_CK(cudaMemsetAsync(fb.counters, 0, 4ull * kCounterWords, stream));
+    // the per-view status words start at zero (counts, error bits): the preprocess and the
+    // classification write into them concurrently
+    FHTGS_CK(cudaMemsetAsync(fb.status, 0, sizeof(FrameStatus) * V, stream));
     n += ks.setup(setups.data(), V, fb.views, stream);
-    n += ks.classify(fp, fb, stream);
     mark(1);
+    // tile classification (one block per view, latency-bound) beside the preprocess: nothing
+    // reads its outputs before the range and work-order stage, where the side stream joins
+    FHTGS_CK(cudaEventRecord(ctx->fork_ev, stream));
+    FHTGS_CK(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
+    n += ks.classify(fp, fb, ctx->side);
+    FHTGS_CK(cudaEventRecord(ctx->join_ev, ctx->side));
     n += ks.preprocess(fp, fb, gs, stream);
     mark(2);
     if (nbp > 0) {
@@ -443,6 +455,7 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     mark(3);
     n += ks.sort(fp, fb, stream);
     mark(4);
+    FHTGS_CK(cudaStreamWaitEvent(stream, ctx->join_ev, 0));
     n += ks.ranges(fp, fb, ctx->n_sms, stream);
     n += ks.order(fp, fb, ctx->n_sms, stream);
     mark(5);
@@ -567,6 +580,13 @@ fhtgs_status fhtgs_context_create(int32_t device, fhtgs_context* out) {
     auto* c = new fhtgs_context_s();
     c->device = device;
     cudaDeviceGetAttribute(&c->n_sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        fhtgs_context_destroy(c);
+        return fail(FHTGS_ERR_CUDA, "context stream/events");
+    }
     *out = c;
     return FHTGS_OK;
 }
@@ -582,6 +602,12 @@ fhtgs_status fhtgs_context_destroy(fhtgs_context ctx) {
         cudaFree(ctx->arena);
     }
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->side) {
+        cudaStreamSynchronize(ctx->side);
+        cudaStreamDestroy(ctx->side);
+    }
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
     delete ctx;
     return FHTGS_OK;
 }

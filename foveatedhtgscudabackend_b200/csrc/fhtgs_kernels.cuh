@@ -226,9 +226,8 @@ __global__ void __launch_bounds__(1024) classify_kernel(FrameParams fp, FrameBuf
         st.n_periphery_large = none ? 0 : nP;
         st.n_quarter_large = nQ;
         st.n_masked_large = none ? nM + nP : nM;
-        st.overflow = 0;
-        st.n_instances = 0;
-        st.n_instances_ref = 0;
+        // overflow and the instance counts were zeroed before the frame: the preprocess,
+        // running beside this kernel, adds to them
     }
 }
 
@@ -1247,8 +1246,11 @@ int launch_sort(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s) {
 // per-large-tile instance ranges from the boundaries of the sorted keys (the boundary rule of
 // extract_instance_ranges_cu, shared_kernels.cuh:133-152; ranges are zeroed beforehand)
 // ------------------------------------------------------------------------------------------
+// Each thread reads 16 bytes of sorted keys at a time (8 u16 or 4 u32 keys; a view's keys start
+// 16-byte aligned: the capacity is a whole number of 4096-key sort tiles) and the key before them.
 template <typename KeyT>
 __global__ void __launch_bounds__(256) ranges_kernel(FrameParams fp, FrameBuffers fb) {
+    constexpr int PER = 16 / static_cast<int>(sizeof(KeyT));
     const int v = blockIdx.y;
     // a view whose sort or staging gave up keeps empty ranges: its sorted values may come from
     // slots that nothing wrote in this frame, and the blend must not read them
@@ -1257,27 +1259,41 @@ __global__ void __launch_bounds__(256) ranges_kernel(FrameParams fp, FrameBuffer
     const KeyT* keys = reinterpret_cast<const KeyT*>(fb.keys[fb.final_buf]) + static_cast<size_t>(v) * fp.cap;
     uint2* r = fb.ranges + static_cast<size_t>(v) * fp.max_large;
     const uint32_t n_large = static_cast<uint32_t>(fb.views[v].n_large);
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < M;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const KeyT k = keys[i];
-        const bool k_ok = static_cast<uint32_t>(k) < n_large;  // sentinels are no tile
-        if (i == 0) {
-            if (k_ok) r[k].x = 0;
+    for (uint64_t c = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c * PER < M;
+         c += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t i0 = c * PER;
+        KeyT k[PER];
+        if (i0 + PER <= M) {
+            const uint4 q = *reinterpret_cast<const uint4*>(keys + i0);
+            memcpy(k, &q, sizeof(q));
         } else {
-            const KeyT prev = keys[i - 1];
-            if (k != prev) {
-                if (static_cast<uint32_t>(prev) < n_large) r[prev].y = static_cast<uint32_t>(i);
-                if (k_ok) r[k].x = static_cast<uint32_t>(i);
-            }
+#pragma unroll
+            for (int j = 0; j < PER; ++j) k[j] = i0 + j < M ? keys[i0 + j] : static_cast<KeyT>(0);
         }
-        if (i == M - 1 && k_ok) r[k].y = static_cast<uint32_t>(M);
+        KeyT prev = i0 > 0 ? keys[i0 - 1] : static_cast<KeyT>(0);
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const uint64_t i = i0 + j;
+            if (i >= M) break;
+            const KeyT kk = k[j];
+            const bool k_ok = static_cast<uint32_t>(kk) < n_large;  // sentinels are no tile
+            if (i == 0) {
+                if (k_ok) r[kk].x = 0;
+            } else if (kk != prev) {
+                if (static_cast<uint32_t>(prev) < n_large) r[prev].y = static_cast<uint32_t>(i);
+                if (k_ok) r[kk].x = static_cast<uint32_t>(i);
+            }
+            if (i == M - 1 && k_ok) r[kk].y = static_cast<uint32_t>(M);
+            prev = kk;
+        }
     }
 }
 
 int launch_ranges(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s) {
     cudaMemsetAsync(fb.ranges, 0, sizeof(uint2) * static_cast<size_t>(fp.max_large) * fp.n_views, s);
     if (fb.sort_tiles == 0) return 0;
-    const int64_t want = (fp.cap + 255) / 256;
+    const int64_t per_thread = fp.key_u32 ? 4 : 8;  // keys of one 16-byte load
+    const int64_t want = (fp.cap + 256 * per_thread - 1) / (256 * per_thread);
     const unsigned nb = static_cast<unsigned>(want < 8 * n_sms ? (want > 0 ? want : 1) : 8 * n_sms);
     dim3 grid(nb, fp.n_views);
     if (fp.key_u32) ranges_kernel<uint32_t><<<grid, 256, 0, s>>>(fp, fb);
@@ -1378,27 +1394,48 @@ __global__ void __launch_bounds__(256) order_hist_kernel(FrameParams fp, FrameBu
         if (hist[k]) atomicAdd(&gh[k], hist[k]);
 }
 
+// Items go to their bucket's run of the work list in rounds of blockDim.x: a block counts its
+// round's items per bucket in shared memory (each item's rank among them), reserves one
+// contiguous place per bucket with a single global atomic, and writes its items there.  (One
+// global atomic per item made the few heavily used buckets' cursors a serial bottleneck.)  The
+// order inside a bucket follows the reservations; it changes the schedule, never a pixel.
 __global__ void __launch_bounds__(256) order_scatter_kernel(FrameParams fp, FrameBuffers fb) {
     __shared__ int pre[kMaxOrderViews];
     __shared__ uint32_t base[kOrderBuckets];
+    __shared__ uint32_t s_cnt[kOrderBuckets];
+    __shared__ uint32_t s_warp[33];
     const int total = items_prefix(fp, fb, pre);
     const uint32_t* gh = fb.counters + 4;
     uint32_t* cursor = fb.counters + 4 + kOrderBuckets;
-    if (threadIdx.x == 0) {  // descending bucket order
-        uint32_t acc = 0;
-        for (int k = kOrderBuckets - 1; k >= 0; --k) {
-            base[k] = acc;
-            acc += gh[k];
-        }
+    {  // each bucket's first place in descending bucket order: a block scan, two buckets a thread
+        static_assert(kOrderBuckets <= 2 * 256, "two buckets per thread of a 256-thread block");
+        const int p0 = 2 * static_cast<int>(threadIdx.x), p1 = p0 + 1;  // places in descending order
+        const uint32_t c0 = p0 < kOrderBuckets ? gh[kOrderBuckets - 1 - p0] : 0u;
+        const uint32_t c1 = p1 < kOrderBuckets ? gh[kOrderBuckets - 1 - p1] : 0u;
+        uint32_t all;
+        const uint32_t e = block_excl_scan<uint32_t>(c0 + c1, all, s_warp);
+        if (p0 < kOrderBuckets) base[kOrderBuckets - 1 - p0] = e;
+        if (p1 < kOrderBuckets) base[kOrderBuckets - 1 - p1] = e + c0;
     }
-    __syncthreads();
     uint32_t* out = fb.work_order[0];
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
-        int v, j;
-        item_of(g, pre, fp.n_views, v, j);
-        uint32_t packed;
-        const int b = item_bucket(fp, fb, v, j, packed);
-        out[base[b] + atomicAdd(&cursor[b], 1u)] = packed;
+    for (int g0 = blockIdx.x * blockDim.x; g0 < total; g0 += gridDim.x * blockDim.x) {
+        for (int k = threadIdx.x; k < kOrderBuckets; k += blockDim.x) s_cnt[k] = 0;
+        __syncthreads();
+        const int g = g0 + static_cast<int>(threadIdx.x);
+        int b = -1;
+        uint32_t packed = 0, local = 0;
+        if (g < total) {
+            int v, j;
+            item_of(g, pre, fp.n_views, v, j);
+            b = item_bucket(fp, fb, v, j, packed);
+            local = atomicAdd(&s_cnt[b], 1u);
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < kOrderBuckets; k += blockDim.x)
+            if (s_cnt[k]) s_cnt[k] = atomicAdd(&cursor[k], s_cnt[k]);
+        __syncthreads();
+        if (b >= 0) out[base[b] + s_cnt[b] + local] = packed;
+        __syncthreads();  // the counts are cleared for the next round
     }
 }
 

@@ -172,7 +172,8 @@ int64_t fhtgs_context_launch_count(fhtgs_context ctx);
 
 /* ---- stage timing ----
  * With profiling on, every frame records CUDA events on its stream between the stages:
- *   0 setup+classify, 1 preprocess, 2 scan+create instances, 3 sort,
+ *   0 setup (status reset, camera gather), 1 preprocess (the tile classification runs beside
+ *   it on a second stream of the context), 2 scan+create instances, 3 sort,
  *   4 tile ranges + blend work order, 5 blend (all tiles), 6 compose.
  * fhtgs_get_stage_times waits for the last frame and returns the milliseconds per stage. */
 #define FHTGS_N_STAGES 7
