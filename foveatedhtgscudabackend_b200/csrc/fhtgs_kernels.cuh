@@ -1986,7 +1986,12 @@ __device__ __forceinline__ float3 blur5(const float3* s, int n, int lx, int ly, 
     return r;
 }
 
-__global__ void __launch_bounds__(256) compose_kernel(FrameParams fp, FrameBuffers fb) {
+// One 64-thread block per non-fovea large tile; each thread produces 4 of its 256 pixels (or
+// one pixel of each of a blended tile's four 8x8 sub-tiles).  Small blocks keep many tiles'
+// sample loads in flight per SM: the stage is bound by the latency of those loads.
+constexpr int kComposeThreads = 64;
+
+__global__ void __launch_bounds__(kComposeThreads) compose_kernel(FrameParams fp, FrameBuffers fb) {
     __shared__ float3 s_samples[4][10 * 10];
     const int v = blockIdx.y;
     const ViewParams& vp = fb.views[v];
@@ -2011,20 +2016,23 @@ __global__ void __launch_bounds__(256) compose_kernel(FrameParams fp, FrameBuffe
         const int max_r = static_cast<int>((static_cast<unsigned>(W) - static_cast<unsigned>(bx) - 1u) / static_cast<unsigned>(kStride));
         const int max_d = static_cast<int>((static_cast<unsigned>(H) - static_cast<unsigned>(by) - 1u) / static_cast<unsigned>(kStride));
         float3* s = s_samples[0];
-        for (int k = tid; k < n * n; k += 256)
+        for (int k = tid; k < n * n; k += kComposeThreads)
             s[k] = grid_sample(vp, ltype, src, chw, bx, by, k % n, k / n, max_r, max_d, ltx, lty, blur);
         __syncthreads();
-        const int lx = tid & 15, ly = tid >> 4;
-        const int px = ox + lx, py = oy + ly;
-        if (px >= W || py >= H) return;
-        if (!blur) {
-            if ((lx % kStride) == 0 && (ly % kStride) == 0) return;
-            const float3 r = bilerp(s, 9, lx, ly);
-            store_rgb(dst, W, H, px, py, chw, __saturatef(r.x), __saturatef(r.y), __saturatef(r.z));
-        } else {
-            float f;
-            const float3 r = blur5(s, 10, lx, ly, f);
-            store_rgb(dst, W, H, px, py, chw, __saturatef(r.x * f), __saturatef(r.y * f), __saturatef(r.z * f));
+        for (int q = 0; q < 4; ++q) {
+            const int p = tid + kComposeThreads * q;
+            const int lx = p & 15, ly = p >> 4;
+            const int px = ox + lx, py = oy + ly;
+            if (px >= W || py >= H) continue;
+            if (!blur) {
+                if ((lx % kStride) == 0 && (ly % kStride) == 0) continue;
+                const float3 r = bilerp(s, 9, lx, ly);
+                store_rgb(dst, W, H, px, py, chw, __saturatef(r.x), __saturatef(r.y), __saturatef(r.z));
+            } else {
+                float f;
+                const float3 r = blur5(s, 10, lx, ly, f);
+                store_rgb(dst, W, H, px, py, chw, __saturatef(r.x * f), __saturatef(r.y * f), __saturatef(r.z * f));
+            }
         }
         return;
     }
@@ -2040,49 +2048,57 @@ __global__ void __launch_bounds__(256) compose_kernel(FrameParams fp, FrameBuffe
         float3* s = s_samples[0];
         if (tid < 25) s[tid] = grid_sample4(vp, src, chw, ox, oy, tid % 5, tid / 5, max_r, max_d, ltx, lty);
         __syncthreads();
-        const int lx = tid & 15, ly = tid >> 4;
-        const int px = ox + lx, py = oy + ly;
-        if (px >= W || py >= H) return;
-        if ((lx % kQuarterStride) == 0 && (ly % kQuarterStride) == 0) return;
-        const float3 r = bilerp<kQuarterStride>(s, 5, lx, ly);
-        store_rgb(dst, W, H, px, py, chw, __saturatef(r.x), __saturatef(r.y), __saturatef(r.z));
+        for (int q = 0; q < 4; ++q) {
+            const int p = tid + kComposeThreads * q;
+            const int lx = p & 15, ly = p >> 4;
+            const int px = ox + lx, py = oy + ly;
+            if (px >= W || py >= H) continue;
+            if ((lx % kQuarterStride) == 0 && (ly % kQuarterStride) == 0) continue;
+            const float3 r = bilerp<kQuarterStride>(s, 5, lx, ly);
+            store_rgb(dst, W, H, px, py, chw, __saturatef(r.x), __saturatef(r.y), __saturatef(r.z));
+        }
         return;
     }
     item -= nQ;
     if (item < nB) {
         const uint32_t lt = fb.work_full[static_cast<size_t>(v) * fp.max_large + st.n_fovea_large + item];
         const int ltx = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)), lty = static_cast<int>(lt / static_cast<uint32_t>(vp.glw));
-        const int g = tid >> 6, t = tid & 63;  // sub-tile group
-        const int ox = ltx * kTileLarge + (g % kStride) * kTileSmall, oy = lty * kTileLarge + (g / kStride) * kTileSmall;
         const int n = blur ? 6 : 5;
-        const int bx = blur ? ox - kStride : ox, by = blur ? oy - kStride : oy;
-        const int max_r = static_cast<int>((static_cast<unsigned>(W) - static_cast<unsigned>(bx) - 1u) / static_cast<unsigned>(kStride));
-        const int max_d = static_cast<int>((static_cast<unsigned>(H) - static_cast<unsigned>(by) - 1u) / static_cast<unsigned>(kStride));
-        float3* s = s_samples[g];
-        for (int k = t; k < n * n; k += 64)
-            s[k] = grid_sample(vp, ltype, src, chw, bx, by, k % n, k / n, max_r, max_d, ltx, lty, blur);
+        // the samples of the four 8x8 sub-tiles g (origins (g % 2, g / 2) x 8 in the tile)
+        for (int k = tid; k < 4 * n * n; k += kComposeThreads) {
+            const int g = k / (n * n), kk = k % (n * n);
+            const int ox = ltx * kTileLarge + (g % kStride) * kTileSmall, oy = lty * kTileLarge + (g / kStride) * kTileSmall;
+            const int bx = blur ? ox - kStride : ox, by = blur ? oy - kStride : oy;
+            const int max_r = static_cast<int>((static_cast<unsigned>(W) - static_cast<unsigned>(bx) - 1u) / static_cast<unsigned>(kStride));
+            const int max_d = static_cast<int>((static_cast<unsigned>(H) - static_cast<unsigned>(by) - 1u) / static_cast<unsigned>(kStride));
+            s_samples[g][kk] = grid_sample(vp, ltype, src, chw, bx, by, kk % n, kk / n, max_r, max_d, ltx, lty, blur);
+        }
         __syncthreads();
-        const int lx = t & 7, ly = t >> 3;
-        const int px = ox + lx, py = oy + ly;
-        if (px >= W || py >= H) return;
-        const float2 dg = vp.gaze_px - make_float2(static_cast<float>(px), static_cast<float>(py));
-        const float bf = clampf((length(dg) - kBlendRadiusPx - kTileLarge) / (kBlendWidthPx - kTileLarge), 0.0f, 1.0f);
-        if (!blur) {
-            if ((lx % kStride) == 0 && (ly % kStride) == 0) return;
-            const float3 r = bilerp(s, 5, lx, ly);
-            const float3 cc = load_rgb(src, W, H, px, py, chw);
-            if (bf > 0.0f)
-                store_rgb(dst, W, H, px, py, chw, __saturatef(r.x * bf + cc.x * (1.0f - bf)),
-                          __saturatef(r.y * bf + cc.y * (1.0f - bf)), __saturatef(r.z * bf + cc.z * (1.0f - bf)));
-        } else {
-            float f;
-            const float3 r = blur5(s, 6, lx, ly, f);
-            const float3 cc = load_rgb(src, W, H, px, py, chw);
-            if (bf > 0.0f)
-                store_rgb(dst, W, H, px, py, chw, __saturatef(cc.x * (1.0f - bf) + r.x * f * bf),
-                          __saturatef(cc.y * (1.0f - bf) + r.y * f * bf), __saturatef(cc.z * (1.0f - bf) + r.z * f * bf));
-            else
-                store_rgb(dst, W, H, px, py, chw, cc.x, cc.y, cc.z);
+        const int lx = tid & 7, ly = tid >> 3;
+        for (int g = 0; g < 4; ++g) {
+            const int ox = ltx * kTileLarge + (g % kStride) * kTileSmall, oy = lty * kTileLarge + (g / kStride) * kTileSmall;
+            const int px = ox + lx, py = oy + ly;
+            if (px >= W || py >= H) continue;
+            const float3* s = s_samples[g];
+            const float2 dg = vp.gaze_px - make_float2(static_cast<float>(px), static_cast<float>(py));
+            const float bf = clampf((length(dg) - kBlendRadiusPx - kTileLarge) / (kBlendWidthPx - kTileLarge), 0.0f, 1.0f);
+            if (!blur) {
+                if ((lx % kStride) == 0 && (ly % kStride) == 0) continue;
+                const float3 r = bilerp(s, 5, lx, ly);
+                const float3 cc = load_rgb(src, W, H, px, py, chw);
+                if (bf > 0.0f)
+                    store_rgb(dst, W, H, px, py, chw, __saturatef(r.x * bf + cc.x * (1.0f - bf)),
+                              __saturatef(r.y * bf + cc.y * (1.0f - bf)), __saturatef(r.z * bf + cc.z * (1.0f - bf)));
+            } else {
+                float f;
+                const float3 r = blur5(s, 6, lx, ly, f);
+                const float3 cc = load_rgb(src, W, H, px, py, chw);
+                if (bf > 0.0f)
+                    store_rgb(dst, W, H, px, py, chw, __saturatef(cc.x * (1.0f - bf) + r.x * f * bf),
+                              __saturatef(cc.y * (1.0f - bf) + r.y * f * bf), __saturatef(cc.z * (1.0f - bf) + r.z * f * bf));
+                else
+                    store_rgb(dst, W, H, px, py, chw, cc.x, cc.y, cc.z);
+            }
         }
         return;
     }
@@ -2091,14 +2107,17 @@ __global__ void __launch_bounds__(256) compose_kernel(FrameParams fp, FrameBuffe
         const uint32_t lt = fb.work_masked[static_cast<size_t>(v) * fp.max_large + item];
         const int ox = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)) * kTileLarge;
         const int oy = static_cast<int>(lt / static_cast<uint32_t>(vp.glw)) * kTileLarge;
-        const int px = ox + (tid & 15), py = oy + (tid >> 4);
-        if (px < W && py < H) store_rgb(dst, W, H, px, py, chw, 0.0f, 0.0f, 0.0f);
+        for (int q = 0; q < 4; ++q) {
+            const int p = tid + kComposeThreads * q;
+            const int px = ox + (p & 15), py = oy + (p >> 4);
+            if (px < W && py < H) store_rgb(dst, W, H, px, py, chw, 0.0f, 0.0f, 0.0f);
+        }
     }
 }
 
 int launch_compose(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s) {
     if (fp.max_large == 0) return 0;
-    compose_kernel<<<dim3(fp.max_large, fp.n_views), 256, 0, s>>>(fp, fb);
+    compose_kernel<<<dim3(fp.max_large, fp.n_views), kComposeThreads, 0, s>>>(fp, fb);
     return 1;
 }
 
