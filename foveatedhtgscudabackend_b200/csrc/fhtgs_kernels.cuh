@@ -1084,7 +1084,7 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok) {
 }
 
 template <typename KeyT, int ITEMS>
-__global__ void __launch_bounds__(kSortThreads, 3) sort_onesweep_kernel(FrameParams fp, FrameBuffers fb, int buf, int pass) {
+__global__ void __launch_bounds__(kSortThreads, 4) sort_onesweep_kernel(FrameParams fp, FrameBuffers fb, int buf, int pass) {
     constexpr int TILE = kSortThreads * ITEMS;
     __shared__ uint32_t s_whist[kSortThreads / 32][kSortBins];  // per-warp counts, then warp starts
     __shared__ uint32_t s_local_start[kSortBins];
