@@ -848,34 +848,37 @@ __global__ void __launch_bounds__(kPrimBlock) create_instances_kernel(FrameParam
         }
     }
     __syncthreads();
-    // Large bounds: the whole block walks them, 256 tiles per step, a block scan of the
-    // per-tile visibility giving each visible tile its slot.
+    // Large bounds: one warp per Gaussian (eight at a time), 32 tiles per step in row-major
+    // bounds order, a ballot of the per-tile visibility giving each visible tile its slot; no
+    // block barrier, so the warps do not wait for one another's Gaussians.
     const uint32_t n_big = s_big_n;
-    for (uint32_t q = 0; q < n_big; ++q) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lanemask_lt = (1u << lane) - 1u;
+    for (uint32_t q = warp; q < n_big; q += kPrimBlock / 32) {
         const uint32_t prim = s_big_prim[q];
         const ushort4 bb = s_big_b[q];
         const uint32_t bw = static_cast<uint32_t>(bb.y - bb.x);
         const uint32_t cnt = static_cast<uint32_t>(bb.w - bb.z) * bw;
         uint64_t w0 = s_big_off[q];
         const uint64_t end = w0 + fb.n_vis[static_cast<size_t>(v) * N + prim];
-        for (uint32_t base = 0; base < cnt; base += kPrimBlock) {
-            const uint32_t k = base + threadIdx.x;
-            uint32_t tile = 0, c = 0;
+        for (uint32_t base = 0; base < cnt; base += 32) {
+            const uint32_t k = base + lane;
+            uint32_t tile = 0;
+            bool c = false;
             if (k < cnt) {
                 tile = (bb.z + k / bw) * glw + bb.x + k % bw;
-                c = tile_visible(vp.vis_mask, tile) ? 1u : 0u;
+                c = tile_visible(vp.vis_mask, tile);
             }
-            uint32_t step;
-            const uint32_t ex = block_excl_scan<uint32_t>(c, step, s_warp);
-            const uint64_t w = w0 + ex;
+            const uint32_t vote = __ballot_sync(0xffffffffu, c);
+            const uint64_t w = w0 + __popc(vote & lanemask_lt);
             if (c && w < lim && w < end) {
                 keys[w] = static_cast<KeyT>(tile);
                 vals[w] = prim;
                 if (onesweep) count_key(s_dhist, passes, tile);
             }
-            w0 += step;
+            w0 += __popc(vote);
         }
-        for (uint64_t w = w0 + threadIdx.x; w < end && w < lim; w += kPrimBlock) {  // see above
+        for (uint64_t w = w0 + lane; w < end && w < lim; w += 32) {  // see above
             keys[w] = static_cast<KeyT>(~KeyT(0));
             vals[w] = kNoPrimitive;
             if (onesweep) count_key(s_dhist, passes, static_cast<KeyT>(~KeyT(0)));
