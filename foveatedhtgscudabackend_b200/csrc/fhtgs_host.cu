@@ -108,6 +108,9 @@ struct fhtgs_context_s {
     long long arena_generation = 0;   // bumped whenever the arena moves (captured graphs go stale)
     bool capturing = false;           // a frame graph is being captured: no profiling events
     fhtgs_tuning tuning{8, 0, kSortItems};
+    float split_share = 0.0f;     // split blend: 0 = off (bit-identical blend)
+    bool split_active = false;    // the last frame ran the split blend
+    int split_recs = 0;           // records per pixel of a later segment; 0 = 8 K + 64
     int64_t cap = 0;              // instance slots per view
     FrameStatus* h_status = nullptr;  // pinned
     int h_status_n = 0;
@@ -141,11 +144,34 @@ struct Layout {
     size_t off_hist, off_dtot, off_ranges, off_map, off_type, off_ltype, off_wf, off_wl, off_wm, off_ctr, off_temp;
     size_t off_order0, off_order1;
     size_t off_ghist, off_look, off_ticket;
+    size_t off_split_of = 0, off_split_list = 0, off_split_ctl = 0, off_split_scratch = 0;
     std::vector<size_t> temp_offsets;
 };
 
+// Split blend sizes of a frame (all zero when the mode is off).
+struct SplitPlan {
+    float share = 0.0f;
+    int blocks = 0, cap = 0, recs = 0, stride = 0;
+};
+
+SplitPlan split_plan(float share, int recs, int K, int blend_blocks_per_sm, int n_sms, int V, int max_large) {
+    SplitPlan sp;
+    if (!(share > 0.0f)) return sp;
+    const int Ki = K >= 32 ? 32 : K >= 16 ? 16 : K >= 8 ? 8 : K >= 4 ? 4 : K >= 2 ? 2 : 1;  // the blend's K
+    const int per_sm = blend_blocks_per_sm > 0 ? std::min(blend_blocks_per_sm, blend_min_blocks(Ki)) : blend_min_blocks(Ki);
+    sp.share = share;
+    sp.blocks = n_sms * per_sm;
+    sp.recs = recs > 0 ? recs : 8 * Ki + 64;  // 20 bytes each
+    sp.stride = split_stride_bytes(Ki, sp.recs);
+    // Segments of about the threshold's length cover at most instances / threshold = blocks /
+    // share list entries; tiles whose reservation does not fit are blended whole.
+    const int64_t bound = static_cast<int64_t>(std::ceil(sp.blocks / static_cast<double>(share))) + 8 * kSplitMaxSegments;
+    sp.cap = static_cast<int>(std::min<int64_t>(bound, static_cast<int64_t>(kSplitMaxSegments) * V * max_large));
+    return sp;
+}
+
 Layout plan(int V, int64_t N, int nbp, int64_t cap, int key_bytes, int sort_tiles, int max_tiles, int max_large,
-            const std::vector<int64_t>& temp_floats) {
+            const std::vector<int64_t>& temp_floats, const SplitPlan& sp) {
     Layout L;
     size_t o = 0;
     auto take = [&](size_t bytes) { size_t at = o; o = align_up(o + std::max<size_t>(bytes, 1)); return at; };
@@ -176,6 +202,12 @@ Layout plan(int V, int64_t N, int nbp, int64_t cap, int key_bytes, int sort_tile
     L.off_look = take(4ull * V * kSortMaxPasses * sort_tiles * kSortBins);
     L.off_ticket = take(4ull * V * kSortMaxPasses);
     for (int64_t f : temp_floats) L.temp_offsets.push_back(f > 0 ? take(4ull * f) : 0);
+    if (sp.cap > 0) {
+        L.off_split_of = take(4ull * V * max_large);
+        L.off_split_list = take(8ull * sp.cap);
+        L.off_split_ctl = take(4ull * sp.cap);
+        L.off_split_scratch = take(static_cast<size_t>(sp.stride) * sp.cap);
+    }
     L.total = o;
     return L;
 }
@@ -262,11 +294,13 @@ int sort_tiles_for(int64_t cap, int sort_items) {
 struct FramePlan {
     std::vector<ViewGeom> geo;
     int max_tiles = 0, max_large = 0, end_bit = 0, key_u32 = 0, nbp = 0, sort_tiles = 0;
+    SplitPlan split;
     Layout L;
 };
 
-FramePlan frame_plan(const fhtgs_primitives* prims, const fhtgs_view* views, int V, const fhtgs_settings* s,
-                     int64_t cap, int sort_items) {
+FramePlan frame_plan(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views, int V,
+                     const fhtgs_settings* s, int64_t cap) {
+    const int sort_items = ctx->tuning.sort_items;
     FramePlan P;
     const int64_t N = prims->n_primitives;
     P.geo.resize(V);
@@ -282,7 +316,9 @@ FramePlan frame_plan(const fhtgs_primitives* prims, const fhtgs_view* views, int
     std::vector<int64_t> temp_floats(V, 0);
     if (s->blur_periphery)
         for (int i = 0; i < V; ++i) temp_floats[i] = 3ll * views[i].width * views[i].height;
-    P.L = plan(V, N, P.nbp, cap, P.key_u32 ? 4 : 2, P.sort_tiles, P.max_tiles, P.max_large, temp_floats);
+    P.split = split_plan(ctx->split_share, ctx->split_recs, s->K, ctx->tuning.blend_blocks_per_sm, ctx->n_sms, V,
+                         P.max_large);
+    P.L = plan(V, N, P.nbp, cap, P.key_u32 ? 4 : 2, P.sort_tiles, P.max_tiles, P.max_large, temp_floats, P.split);
     return P;
 }
 
@@ -297,7 +333,7 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     const int64_t N = prims->n_primitives;
     if (ctx->cap <= 0) ctx->cap = estimate_capacity(N);
     const int64_t cap = ctx->cap;
-    FramePlan P = frame_plan(prims, views, V, s, cap, ctx->tuning.sort_items);
+    FramePlan P = frame_plan(ctx, prims, views, V, s, cap);
     const std::vector<ViewGeom>& geo = P.geo;
     const int max_tiles = P.max_tiles, max_large = P.max_large, end_bit = P.end_bit, key_u32 = P.key_u32;
     const int nbp = P.nbp, sort_tiles = P.sort_tiles;
@@ -372,6 +408,18 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
         fb.sort_ghist = reinterpret_cast<uint32_t*>(A + L.off_ghist);
         fb.sort_look = reinterpret_cast<uint32_t*>(A + L.off_look);
         fb.sort_ticket = reinterpret_cast<uint32_t*>(A + L.off_ticket);
+    }
+    SplitArgs sa{};
+    if (P.split.cap > 0) {
+        sa.share = P.split.share;
+        sa.blocks = P.split.blocks;
+        sa.cap = P.split.cap;
+        sa.recs = P.split.recs;
+        sa.stride = P.split.stride;
+        sa.of = reinterpret_cast<uint32_t*>(A + L.off_split_of);
+        sa.list = reinterpret_cast<uint2*>(A + L.off_split_list);
+        sa.ctl = reinterpret_cast<uint32_t*>(A + L.off_split_ctl);
+        sa.scratch = A + L.off_split_scratch;
     }
 
     std::vector<ViewSetup> setups(V);
@@ -457,9 +505,9 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     mark(4);
     FHTGS_CK(cudaStreamWaitEvent(stream, ctx->join_ev, 0));
     n += ks.ranges(fp, fb, ctx->n_sms, stream);
-    n += ks.order(fp, fb, ctx->n_sms, stream);
+    n += ks.order(fp, fb, sa, ctx->n_sms, stream);
     mark(5);
-    n += ks.blend(fp, fb, ctx->n_sms, stream, nullptr);
+    n += ks.blend(fp, fb, sa, ctx->n_sms, stream, nullptr);
     mark(6);
     n += ks.compose(fp, fb, stream);
     mark(7);
@@ -470,6 +518,7 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
     ctx->have_frame = true;
     ctx->fp = fp;
     ctx->fb = fb;
+    ctx->split_active = sa.cap > 0;
     ctx->geo = geo;
     ctx->views.assign(views, views + V);
     ctx->frame_foveation = s->foveation;
@@ -535,7 +584,7 @@ fhtgs_status enqueue_frame(fhtgs_context ctx, const fhtgs_primitives* prims, con
 
 size_t frame_arena_need(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views, int n_views,
                         const fhtgs_settings* s, int64_t cap) {
-    const size_t total = frame_plan(prims, views, n_views, s, cap, ctx->tuning.sort_items).L.total;
+    const size_t total = frame_plan(ctx, prims, views, n_views, s, cap).L.total;
     if (total <= ctx->arena_bytes) return ctx->arena_bytes;
     return align_up(total + total / 8);  // what ensure_arena allocates
 }
@@ -625,7 +674,9 @@ fhtgs_status fhtgs_context_reserve(fhtgs_context ctx, int32_t n_primitives, int3
     const int nbp = (n_primitives + kPrimBlock - 1) / kPrimBlock;
     std::vector<int64_t> temp(n_views, 3ll * max_width * max_height);
     Layout L = plan(n_views, n_primitives, nbp, ctx->cap, end_bit_of(n_tiles + 1) > 16 ? 4 : 2,
-                    sort_tiles_for(ctx->cap, kSortItemsMin), n_tiles, n_large, temp);
+                    sort_tiles_for(ctx->cap, kSortItemsMin), n_tiles, n_large, temp,
+                    split_plan(ctx->split_share, ctx->split_recs, 32, ctx->tuning.blend_blocks_per_sm, ctx->n_sms,
+                               n_views, n_large));
     return ensure_arena(ctx, L.total);
 }
 
@@ -805,6 +856,34 @@ fhtgs_status fhtgs_context_set_tuning(fhtgs_context ctx, const fhtgs_tuning* t) 
     return FHTGS_OK;
 }
 
+fhtgs_status fhtgs_context_set_blend_split(fhtgs_context ctx, float segment_share, int32_t records) {
+    if (!ctx) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
+    if (!(segment_share == 0.0f || (segment_share >= 0.05f && segment_share <= 8.0f)))
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "segment_share must be 0 (off) or in [0.05, 8]");
+    if (records < 0 || records > 256) return fail(FHTGS_ERR_INVALID_ARGUMENT, "records must be in [0, 256]");
+    ctx->split_share = segment_share;
+    ctx->split_recs = records;
+    return FHTGS_OK;
+}
+
+fhtgs_status fhtgs_context_get_blend_split_stats(fhtgs_context ctx, int32_t* split_tiles, int32_t* segments,
+                                                 int32_t* whole_fallbacks, int32_t* max_records) {
+    if (!ctx || !split_tiles || !segments || !whole_fallbacks || !max_records)
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
+    if (!ctx->have_frame) return fail(FHTGS_ERR_NOT_READY, "no frame rendered yet");
+    *split_tiles = *segments = *whole_fallbacks = *max_records = 0;
+    if (!ctx->split_active) return FHTGS_OK;
+    FHTGS_CK(cudaSetDevice(ctx->device));
+    uint32_t c[kCtrHist];
+    FHTGS_CK(cudaMemcpyAsync(c, ctx->fb.counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+    FHTGS_CK(cudaStreamSynchronize(ctx->stream));
+    *split_tiles = static_cast<int32_t>(c[kCtrSplitTiles]);
+    *segments = static_cast<int32_t>(c[kCtrSplitSegs]);
+    *whole_fallbacks = static_cast<int32_t>(c[kCtrSplitFallback]);
+    *max_records = static_cast<int32_t>(c[kCtrSplitRecMax]);
+    return FHTGS_OK;
+}
+
 fhtgs_status fhtgs_context_get_tuning(fhtgs_context ctx, fhtgs_tuning* t) {
     if (!ctx || !t) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
     *t = ctx->tuning;
@@ -909,6 +988,7 @@ struct fhtgs_frame_graph_s {
     std::vector<ViewGeom> geo;
     std::vector<fhtgs_view> views;
     int frame_foveation = 0;
+    bool split_active = false;
 };
 
 fhtgs_status fhtgs_frame_graph_create(fhtgs_context ctx, const fhtgs_primitives* prims, const fhtgs_view* views,
@@ -969,6 +1049,7 @@ fhtgs_status fhtgs_frame_graph_create(fhtgs_context ctx, const fhtgs_primitives*
     g->launches_per_frame = per_frame;
     g->fp = ctx->fp;
     g->fb = ctx->fb;
+    g->split_active = ctx->split_active;
     g->geo = ctx->geo;
     g->views = ctx->views;
     g->frame_foveation = ctx->frame_foveation;
@@ -987,6 +1068,7 @@ fhtgs_status fhtgs_frame_graph_launch(fhtgs_frame_graph g, void* stream_) {
     ctx->have_frame = true;
     ctx->fp = g->fp;
     ctx->fb = g->fb;
+    ctx->split_active = g->split_active;
     ctx->geo = g->geo;
     ctx->views = g->views;
     ctx->frame_foveation = g->frame_foveation;

@@ -1089,6 +1089,7 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok) {
 template <typename KeyT, int ITEMS>
 __global__ void __launch_bounds__(kSortThreads, 4) sort_onesweep_kernel(FrameParams fp, FrameBuffers fb, int buf, int pass) {
     constexpr int TILE = kSortThreads * ITEMS;
+    static_assert(32 * ITEMS < 65536, "a warp's ranks are packed as 16-bit fields");
     __shared__ uint32_t s_whist[kSortThreads / 32][kSortBins];  // per-warp counts, then warp starts
     __shared__ uint32_t s_local_start[kSortBins];
     __shared__ uint32_t s_global_start[kSortBins];
@@ -1118,7 +1119,9 @@ __global__ void __launch_bounds__(kSortThreads, 4) sort_onesweep_kernel(FramePar
     const uint32_t wbase = static_cast<uint32_t>(warp) * 32 * ITEMS + lane;
     KeyT k_reg[ITEMS];
     uint32_t v_reg[ITEMS];
-    uint32_t rank[ITEMS];  // same-digit keys of this warp before the key
+    // same-digit keys of this warp before the key, two 16-bit ranks per word (a warp ranks at
+    // most 32 x ITEMS keys)
+    uint32_t rank2[(ITEMS + 1) / 2] = {};
 #pragma unroll
     for (int it = 0; it < ITEMS; ++it) {
         const uint32_t idx = wbase + it * 32;
@@ -1133,7 +1136,7 @@ __global__ void __launch_bounds__(kSortThreads, 4) sort_onesweep_kernel(FramePar
         const uint32_t peers = digit_peers(d, ok);
         const uint32_t base = ok ? s_whist[warp][d] : 0u;
         __syncwarp();
-        rank[it] = base + __popc(peers & lanemask_lt);
+        rank2[it >> 1] |= (base + __popc(peers & lanemask_lt)) << (16 * (it & 1));
         if (ok && lane == __ffs(peers) - 1) s_whist[warp][d] = base + __popc(peers);
         __syncwarp();
     }
@@ -1185,7 +1188,7 @@ __global__ void __launch_bounds__(kSortThreads, 4) sort_onesweep_kernel(FramePar
     for (int it = 0; it < ITEMS; ++it) {
         if (wbase + it * 32 < n_here) {
             const uint32_t dd = (static_cast<uint32_t>(k_reg[it]) >> shift) & (kSortBins - 1);
-            const uint32_t p = s_whist[warp][dd] + rank[it];
+            const uint32_t p = s_whist[warp][dd] + ((rank2[it >> 1] >> (16 * (it & 1))) & 0xffffu);
             s_keys[p] = k_reg[it];
             s_vals[p] = v_reg[it];
         }
@@ -1313,6 +1316,7 @@ int launch_ranges(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cuda
 // buckets are served heaviest first, so that long serial per-pixel chains start early.
 // ------------------------------------------------------------------------------------------
 constexpr uint32_t kItemLowres = 1u << 23;
+constexpr uint32_t kItemSplit = ~0u;  // a place of a tile the split blend renders (view 255 never exists)
 
 __device__ __forceinline__ int items_of_view(const FrameStatus& st) {
     return static_cast<int>(st.n_fovea_large + st.n_blended_large + st.n_periphery_large + st.n_quarter_large);
@@ -1354,12 +1358,32 @@ __device__ __forceinline__ uint32_t item_cost(const FrameParams& fp, const Frame
 // cost bucket, so that the descending scatter lists every full-resolution tile first (all 8
 // warps of a block busy), then the periphery tiles, then the quarter tiles, each class heaviest
 // first; a strided tile then never holds a block that full-resolution work is waiting for.
-__device__ __forceinline__ int item_bucket(const FrameParams& fp, const FrameBuffers& fb, int v, int j, uint32_t& packed) {
-    const uint32_t cost = item_cost(fp, fb, v, j, packed);
+__device__ __forceinline__ int item_bucket(const FrameParams& fp, const FrameBuffers& fb, int v, int j, uint32_t& packed,
+                                           uint32_t& cost) {
+    cost = item_cost(fp, fb, v, j, packed);
     const FrameStatus& st = fb.status[v];
     const int n_full = static_cast<int>(st.n_fovea_large + st.n_blended_large);
     const int cls = j < n_full ? 2 : (j - n_full) < static_cast<int>(st.n_periphery_large) ? 1 : 0;
     return cls * kCostBuckets + cost_bucket(cost);
+}
+
+// Split blend: the list length above which a full-resolution tile is split, share x the
+// frame's instances per blend block (0 when the mode is off).
+__device__ __forceinline__ uint32_t split_threshold(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp) {
+    if (!(sp.share > 0.0f) || sp.of == nullptr) return 0u;
+    uint64_t m = 0;
+    for (int v = 0; v < fp.n_views; ++v) m += view_count(fp, fb, v);
+    const double t = static_cast<double>(sp.share) * static_cast<double>(m) / static_cast<double>(sp.blocks);
+    return t < 256.0 ? 256u : t > 4.0e9 ? 4000000000u : static_cast<uint32_t>(t);
+}
+
+// Reserves S consecutive segments for a split tile (one atomic).  A reservation that does not
+// fit the scratch fails and marks the slots it reached below the capacity unused.
+__device__ __forceinline__ bool split_reserve(const FrameBuffers& fb, const SplitArgs& sp, uint32_t S, uint32_t& seg0) {
+    seg0 = atomicAdd(&fb.counters[kCtrSplitSegs], S);
+    if (seg0 + S <= static_cast<uint32_t>(sp.cap)) return true;
+    for (uint32_t k = seg0; k < static_cast<uint32_t>(sp.cap); ++k) sp.list[k] = make_uint2(0u, ~0u);
+    return false;
 }
 
 constexpr int kMaxOrderViews = 1024;
@@ -1379,20 +1403,40 @@ __device__ __forceinline__ int items_prefix(const FrameParams& fp, const FrameBu
     return s_total;
 }
 
-__global__ void __launch_bounds__(256) order_hist_kernel(FrameParams fp, FrameBuffers fb) {
+// Also decides which full-resolution tiles the split blend splits (their places in the work
+// list hold kItemSplit, and their segments go to the split list) and clears the split tickets.
+__global__ void __launch_bounds__(256) order_hist_kernel(FrameParams fp, FrameBuffers fb, SplitArgs sp) {
     __shared__ int pre[kMaxOrderViews];
     __shared__ uint32_t hist[kOrderBuckets];
+    __shared__ uint32_t s_split_len;
     const int total = items_prefix(fp, fb, pre);
     for (int k = threadIdx.x; k < kOrderBuckets; k += blockDim.x) hist[k] = 0;
+    if (threadIdx.x == 0) s_split_len = split_threshold(fp, fb, sp);
     __syncthreads();
+    const uint32_t split_len = s_split_len;
+    if (split_len > 0)
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < sp.cap; k += gridDim.x * blockDim.x) sp.ctl[k] = 0u;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
         int v, j;
         item_of(g, pre, fp.n_views, v, j);
-        uint32_t packed;
-        atomicAdd(&hist[item_bucket(fp, fb, v, j, packed)], 1u);
+        uint32_t packed, cost;
+        const int b = item_bucket(fp, fb, v, j, packed, cost);
+        if (split_len > 0 && b >= 2 * kCostBuckets) {  // a full-resolution tile: cost = 8 x length
+            const uint32_t len = cost / 8u;
+            uint32_t tag = ~0u, seg0;
+            if (len > split_len) {
+                const uint32_t S = min(static_cast<uint32_t>(kSplitMaxSegments), (len + split_len - 1) / split_len);
+                if (split_reserve(fb, sp, S, seg0)) {
+                    tag = seg0 | (S << 28);
+                    atomicAdd(&fb.counters[kCtrSplitTiles], 1u);
+                }
+            }
+            sp.of[static_cast<size_t>(v) * fp.max_large + j] = tag;
+        }
+        atomicAdd(&hist[b], 1u);
     }
     __syncthreads();
-    uint32_t* gh = fb.counters + 4;
+    uint32_t* gh = fb.counters + kCtrHist;
     for (int k = threadIdx.x; k < kOrderBuckets; k += blockDim.x)
         if (hist[k]) atomicAdd(&gh[k], hist[k]);
 }
@@ -1402,14 +1446,14 @@ __global__ void __launch_bounds__(256) order_hist_kernel(FrameParams fp, FrameBu
 // contiguous place per bucket with a single global atomic, and writes its items there.  (One
 // global atomic per item made the few heavily used buckets' cursors a serial bottleneck.)  The
 // order inside a bucket follows the reservations; it changes the schedule, never a pixel.
-__global__ void __launch_bounds__(256) order_scatter_kernel(FrameParams fp, FrameBuffers fb) {
+__global__ void __launch_bounds__(256) order_scatter_kernel(FrameParams fp, FrameBuffers fb, SplitArgs sp) {
     __shared__ int pre[kMaxOrderViews];
     __shared__ uint32_t base[kOrderBuckets];
     __shared__ uint32_t s_cnt[kOrderBuckets];
     __shared__ uint32_t s_warp[33];
     const int total = items_prefix(fp, fb, pre);
-    const uint32_t* gh = fb.counters + 4;
-    uint32_t* cursor = fb.counters + 4 + kOrderBuckets;
+    const uint32_t* gh = fb.counters + kCtrHist;
+    uint32_t* cursor = fb.counters + kCtrHist + kOrderBuckets;
     {  // each bucket's first place in descending bucket order: a block scan, two buckets a thread
         static_assert(kOrderBuckets <= 2 * 256, "two buckets per thread of a 256-thread block");
         const int p0 = 2 * static_cast<int>(threadIdx.x), p1 = p0 + 1;  // places in descending order
@@ -1430,8 +1474,17 @@ __global__ void __launch_bounds__(256) order_scatter_kernel(FrameParams fp, Fram
         if (g < total) {
             int v, j;
             item_of(g, pre, fp.n_views, v, j);
-            b = item_bucket(fp, fb, v, j, packed);
-            local = atomicAdd(&s_cnt[b], 1u);
+            uint32_t cost;
+            b = item_bucket(fp, fb, v, j, packed, cost);
+            if (sp.of != nullptr && sp.share > 0.0f && b >= 2 * kCostBuckets) {
+                const uint32_t tag = sp.of[static_cast<size_t>(v) * fp.max_large + j];
+                if (tag != ~0u) {  // a split tile: its segments go to the split list
+                    const uint32_t seg0 = tag & 0x0fffffffu, S = tag >> 28;
+                    for (uint32_t k = 0; k < S; ++k) sp.list[seg0 + k] = make_uint2(packed, tag);
+                    packed = kItemSplit;
+                }
+            }
+            if (b >= 0) local = atomicAdd(&s_cnt[b], 1u);
         }
         __syncthreads();
         for (int k = threadIdx.x; k < kOrderBuckets; k += blockDim.x)
@@ -1442,12 +1495,12 @@ __global__ void __launch_bounds__(256) order_scatter_kernel(FrameParams fp, Fram
     }
 }
 
-int launch_order(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s) {
+int launch_order(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp, int n_sms, cudaStream_t s) {
     const int per_view = fp.max_large;
     int blocks = (fp.n_views * per_view + 255) / 256;
     blocks = blocks < 2 * n_sms ? (blocks > 0 ? blocks : 1) : 2 * n_sms;
-    order_hist_kernel<<<blocks, 256, 0, s>>>(fp, fb);
-    order_scatter_kernel<<<blocks, 256, 0, s>>>(fp, fb);
+    order_hist_kernel<<<blocks, 256, 0, s>>>(fp, fb, sp);
+    order_scatter_kernel<<<blocks, 256, 0, s>>>(fp, fb, sp);
     return 2;
 }
 
@@ -1625,9 +1678,6 @@ __device__ __forceinline__ bool conic_meets_rect(const Conic& q, float ax0, floa
 // One block renders one 16x16 area.  LOWRES: 64 threads sample it at stride 2 (periphery);
 // otherwise 256 threads render it at full resolution (fovea / blended).  Warp w covers an
 // 8-wide, 4-high block of samples.
-// Resident blocks per SM the register allocation has to allow: the K-buffer (2 K registers)
-// dominates for large K.
-__host__ __device__ constexpr int blend_min_blocks(int K) { return K >= 32 ? 2 : K >= 16 ? 3 : 4; }
 
 struct BlendSmem {
     float4* p1;
@@ -1646,9 +1696,50 @@ struct BlendSmem {
 // the warp rectangles, and every warp then walks only its own compacted list, in list order.
 // The warp shape only changes which pairs are culled (pairs that cannot pass the alpha test),
 // never a pixel's arithmetic.  The tile layout is a compile-time constant of each class.
-template <int K, int RW, int CLS>
+// A segment of a split tile's list (SEG instantiation only).  mode 0: the whole list, resolved
+// as usual (a split tile blended whole); mode 1: the first segment, whose K-buffer, tail and
+// transmittance go to its scratch; mode 2: a later segment, walked from an empty K-buffer: every
+// fragment that enters it is recorded (depth, premultiplied colour) instead of being blended,
+// and the tail holds only the fragments that never entered it.
+struct SegWalk {
+    uint32_t s, S;
+    int mode;
+    int recs;  // records kept per pixel (mode 2)
+    char* scratch;
+};
+
+// Resolves one pixel from its K-buffer, tail and tail transmittance: the split blend's merge
+// (the same steps as the end of blend_tile).
+template <int K>
+__device__ __forceinline__ void blend_resolve(const FrameParams& fp, const ViewParams& vp, const Frag (&core)[K],
+                                              const float4 tail, const float tail_T, float pixel_x, float pixel_y,
+                                              float* out, int px_i, int py_i) {
+    float3 rgb = make_float3(0.0f, 0.0f, 0.0f);
+    float Tc = 1.0f;
+#pragma unroll
+    for (int k = 0; k < K && Tc >= kTransmittanceThreshold; ++k) {
+        const float4 c = unpack_rgba(core[k].color);
+        rgb += Tc * xyz(c);
+        Tc *= 1.0f - c.w;
+    }
+    if (Tc >= kTransmittanceThreshold && tail.w >= kMinAlpha) {
+        const float wt = Tc * (1.0f - tail_T);
+        rgb += wt * (1.0f / tail.w) * xyz(tail);
+    }
+    if (fp.bg_type != 0) {
+        const float wb = Tc * tail_T;
+        if (wb >= kTransmittanceThreshold) {
+            if (fp.bg_type == 1) rgb += wb * eval_sh_background(vp, fp.bg_data, pixel_x, pixel_y);
+            else rgb += wb * eval_tex_background(vp, fp.bg_data, fp.tex_w, fp.tex_h, fp.bg_type == 3, pixel_x, pixel_y);
+        }
+    }
+    store_rgb(out, vp.width, vp.height, px_i, py_i, fp.to_chw != 0, __saturatef(rgb.x), __saturatef(rgb.y),
+              __saturatef(rgb.z));
+}
+
+template <int K, int RW, int CLS, int SEG = 0>
 __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuffers& fb, uint32_t packed,
-                                        const BlendSmem& sm) {
+                                        const BlendSmem& sm, const SegWalk sw = SegWalk{0u, 1u, 0, 0, nullptr}) {
     constexpr int NT = 256;
     constexpr int NW = NT / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1677,9 +1768,16 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
     const bool inside = warp < n_warps && (lane >> rw_bits) < rh_used && px_i < vp.width && py_i < vp.height;
     const float pixel_x = __uint2float_rn(static_cast<uint32_t>(px_i));
     const float pixel_y = __uint2float_rn(static_cast<uint32_t>(py_i));
-    const uint2 range = fb.ranges[static_cast<size_t>(v) * fp.max_large + lt];
+    uint2 range = fb.ranges[static_cast<size_t>(v) * fp.max_large + lt];
+    if constexpr (SEG != 0) {  // segment s of S equal parts of the list
+        const uint64_t len = range.y > range.x ? range.y - range.x : 0u;
+        const uint32_t lo = range.x + static_cast<uint32_t>(len * sw.s / sw.S);
+        const uint32_t hi = range.x + static_cast<uint32_t>(len * (sw.s + 1u) / sw.S);
+        range = make_uint2(lo, hi);
+    }
     const uint32_t* vals = fb.vals[fb.final_buf] + static_cast<size_t>(v) * fp.cap;
     const float4* rec = fb.rec + 4 * static_cast<size_t>(v) * fp.n_prims;
+    uint32_t n_rec = 0;  // SEG mode 2: fragments that entered the K-buffer
 
     float tail_T = 1.0f;
     float4 tail = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -1763,6 +1861,15 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
                 const float3 ep = cross(d, m) * den_rcp;
                 const float depth = dot(xyz(VPMT4), ep) + VPMT4.w;
                 if (cand && depth < core[K - 1].depth) {
+                    if constexpr (SEG != 0) {
+                        if (sw.mode == 2) {  // recorded; the merge decides what it does
+                            if (n_rec < static_cast<uint32_t>(sw.recs)) {
+                                reinterpret_cast<float*>(sw.scratch + 6 * 4 * NT)[n_rec * NT + tid] = depth;
+                                reinterpret_cast<float4*>(sw.scratch + (6 + sw.recs) * 4 * NT)[n_rec * NT + tid] = pm;
+                            }
+                            ++n_rec;
+                        }
+                    }
                     Frag f;
                     f.depth = depth;
                     f.color = pack_rgba(pm);
@@ -1775,6 +1882,9 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
                         }
                     }
                     pm = unpack_rgba(f.color);
+                    if constexpr (SEG != 0) {
+                        if (sw.mode == 2) pm = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // adds nothing below
+                    }
                 }
             }
             if (frag) {
@@ -1782,6 +1892,26 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
                 tail += pm;
                 tail_T *= pt;
             }
+        }
+    }
+    if constexpr (SEG != 0) {
+        if (sw.mode == 1) {
+            float* cd = reinterpret_cast<float*>(sw.scratch);
+            uint32_t* cc = reinterpret_cast<uint32_t*>(sw.scratch + K * 4 * NT);
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                cd[k * NT + tid] = core[k].depth;
+                cc[k * NT + tid] = core[k].color;
+            }
+            reinterpret_cast<float4*>(sw.scratch + 2 * K * 4 * NT)[tid] = tail;
+            reinterpret_cast<float*>(sw.scratch + (2 * K + 4) * 4 * NT)[tid] = tail_T;
+            return;
+        }
+        if (sw.mode == 2) {
+            reinterpret_cast<uint32_t*>(sw.scratch)[tid] = n_rec;
+            reinterpret_cast<float4*>(sw.scratch + 4 * NT)[tid] = tail;
+            reinterpret_cast<float*>(sw.scratch + 5 * 4 * NT)[tid] = tail_T;
+            return;
         }
     }
     if (inside) {
@@ -1810,10 +1940,129 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
     }
 }
 
+// One segment of a split full-resolution tile (split list entry g).  The last of the tile's
+// segments to finish merges them: per pixel it starts from the first segment's K-buffer and
+// tail, and replays every later segment's records in list order with the K-buffer's own
+// insertion rule.  A fragment that never entered its segment's (initially empty) K-buffer can
+// never enter the true one, whose K-th depth is never larger, so the replay reproduces every
+// insertion and eviction of the serial walk exactly; only the tail sums and the transmittance
+// products are combined in a different order.  If some pixel recorded more fragments than the
+// scratch holds, the merging block blends the whole tile serially instead.
+template <int K, int RW>
+__device__ __forceinline__ void blend_split_segment(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp,
+                                                    uint32_t g, const BlendSmem& sm) {
+    constexpr int NT = 256;
+    __shared__ int s_last;
+    const int tid = threadIdx.x;
+    const uint2 e = sp.list[g];
+    if (e.y == ~0u) return;  // a slot of a reservation that did not fit
+    const uint32_t packed = e.x, seg0 = e.y & 0x0fffffffu, S = e.y >> 28, s = g - seg0;
+    const size_t stride = static_cast<size_t>(sp.stride);
+    blend_tile<K, RW, 0, 1>(fp, fb, packed, sm, SegWalk{s, S, s == 0 ? 1 : 2, sp.recs, sp.scratch + g * stride});
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(&sp.ctl[seg0], 1u) == S - 1u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const char* base = sp.scratch + seg0 * stride;
+    const int R = sp.recs;
+    uint32_t most = 0;
+    for (uint32_t k = 1; k < S; ++k) most = max(most, __ldcg(reinterpret_cast<const uint32_t*>(base + k * stride) + tid));
+    const uint32_t warp_most = __reduce_max_sync(0xffffffffu, most);
+    if ((tid & 31) == 0 && warp_most > 0) atomicMax(&fb.counters[kCtrSplitRecMax], warp_most);
+    if (__syncthreads_or(most > static_cast<uint32_t>(R))) {
+        if (tid == 0) atomicAdd(&fb.counters[kCtrSplitFallback], 1u);
+        blend_tile<K, RW, 0, 1>(fp, fb, packed, sm, SegWalk{0u, 1u, 0, 0, nullptr});
+        return;
+    }
+    // this thread's pixel (the full-resolution layout of blend_tile)
+    const int lane = tid & 31, warp = tid >> 5;
+    const int v = static_cast<int>(packed >> 24);
+    const int item = static_cast<int>(packed & (kItemLowres - 1u));
+    const ViewParams& vp = fb.views[v];
+    const uint32_t lt = fb.work_full[static_cast<size_t>(v) * fp.max_large + item];
+    const bool is_fovea = static_cast<uint32_t>(item) < fb.status[v].n_fovea_large;
+    constexpr int rw_bits = RW == 4 ? 2 : RW == 8 ? 3 : 4;
+    constexpr int rw = 1 << rw_bits, rh = 32 >> rw_bits;
+    constexpr int wx_bits = 4 - rw_bits;
+    const int px_i = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)) * kTileLarge + (warp & ((1 << wx_bits) - 1)) * rw + (lane & (rw - 1));
+    const int py_i = static_cast<int>(lt / static_cast<uint32_t>(vp.glw)) * kTileLarge + (warp >> wx_bits) * rh + (lane >> rw_bits);
+    if (px_i >= vp.width || py_i >= vp.height) return;
+    Frag core[K];
+    const float* cd = reinterpret_cast<const float*>(base);
+    const uint32_t* cc = reinterpret_cast<const uint32_t*>(base + K * 4 * NT);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        core[k].depth = __ldcg(cd + k * NT + tid);
+        core[k].color = __ldcg(cc + k * NT + tid);
+    }
+    float4 tail = __ldcg(reinterpret_cast<const float4*>(base + 2 * K * 4 * NT) + tid);
+    float tail_T = __ldcg(reinterpret_cast<const float*>(base + (2 * K + 4) * 4 * NT) + tid);
+    for (uint32_t k = 1; k < S; ++k) {
+        const char* b = base + k * stride;
+        const uint32_t n = __ldcg(reinterpret_cast<const uint32_t*>(b) + tid);
+        tail += __ldcg(reinterpret_cast<const float4*>(b + 4 * NT) + tid);
+        tail_T *= __ldcg(reinterpret_cast<const float*>(b + 5 * 4 * NT) + tid);
+        const float* rd = reinterpret_cast<const float*>(b + 6 * 4 * NT);
+        const float4* rp = reinterpret_cast<const float4*>(b + (6 + R) * 4 * NT);
+#pragma unroll 4
+        for (uint32_t r = 0; r < n; ++r) {
+            const float depth = __ldcg(rd + r * NT + tid);
+            float4 pm = __ldcg(rp + r * NT + tid);
+            if (depth < core[K - 1].depth) {
+                Frag f;
+                f.depth = depth;
+                f.color = pack_rgba(pm);
+#pragma unroll
+                for (int q = 0; q < K; ++q) {
+                    if (f.depth < core[q].depth) {
+                        const Frag tf = core[q];
+                        core[q] = f;
+                        f = tf;
+                    }
+                }
+                pm = unpack_rgba(f.color);
+            }
+            tail += pm;
+            tail_T *= 1.0f - pm.w;
+        }
+    }
+    blend_resolve<K>(fp, vp, core, tail, tail_T, __uint2float_rn(static_cast<uint32_t>(px_i)),
+                     __uint2float_rn(static_cast<uint32_t>(py_i)), is_fovea ? vp.image : vp.work, px_i, py_i);
+}
+
+// The split segments of a frame, longest lists first, on persistent blocks; it lets the blend of
+// the other tiles (launched after it as its programmatic dependent) start at once, so that
+// those blocks take the SMs as this kernel's blocks run out of segments.
+template <int K, int RW>
+__global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_split_kernel(FrameParams fp, FrameBuffers fb,
+                                                                              SplitArgs sp) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    constexpr int NT = 256;
+    constexpr int NW = NT / 32;
+    __shared__ float4 s_p1[NT], s_p2[NT], s_p4[NT], s_rgba[NT];
+    __shared__ uint32_t s_mask[NT];
+    __shared__ uint8_t s_list[NW][NT];
+    __shared__ int s_item;
+    const BlendSmem sm{s_p1, s_p2, s_p4, s_rgba, s_mask, s_list};
+    const uint32_t n_seg = min(fb.counters[kCtrSplitSegs], static_cast<uint32_t>(sp.cap));
+    for (;;) {
+        if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(&fb.counters[kCtrSplitNext], 1u));
+        __syncthreads();
+        const uint32_t g = static_cast<uint32_t>(s_item);
+        __syncthreads();
+        if (g >= n_seg) break;
+        blend_split_segment<K, RW>(fp, fb, sp, g, sm);
+    }
+}
+
 // One persistent kernel blends every tile of every view.  The work list holds the full-resolution
 // tiles, then the periphery tiles, then the quarter tiles, each class heaviest first; blocks take
 // items class by class, each class with its own compiled tile code.
-template <int K, int RW>
+// SPLIT: launched after blend_split_kernel as its programmatic dependent (its own instantiation,
+// so that the default path's code is not touched by the split blend's).
+template <int K, int RW, bool SPLIT>
 __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FrameParams fp, FrameBuffers fb) {
     constexpr int NT = 256;
     constexpr int NW = NT / 32;
@@ -1837,7 +2086,12 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
         const int g = s_item;
         __syncthreads();
         if (g >= n_full) break;
-        blend_tile<K, RW, 0>(fp, fb, order[g], sm);
+        if constexpr (SPLIT) {
+            const uint32_t it = order[g];
+            if (it != kItemSplit) blend_tile<K, RW, 0>(fp, fb, it, sm);  // else the split kernel's
+        } else {
+            blend_tile<K, RW, 0>(fp, fb, order[g], sm);
+        }
     }
     for (;;) {  // periphery tiles
         if (tid == 0) s_item = static_cast<int>(atomicAdd(&fb.counters[1], 1u));
@@ -1855,36 +2109,60 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
         if (g >= n_quarter) break;
         blend_tile<K, RW, 2>(fp, fb, order[n_full + n_half + g], sm);
     }
+    // this grid completes only after the split kernel's has
+    if constexpr (SPLIT) asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 template <int K, int RW>
-int launch_blend_kr(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid) {
-    static int occ = -1;  // per instantiation, queried once
-    if (occ < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, blend_kernel<K, RW>, 256, 0);
+int launch_blend_kr(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp, int n_sms, cudaStream_t s,
+                    cudaEvent_t mid) {
+    static int occ = -1, occ_split = -1;  // per instantiation, queried once
+    if (occ < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, blend_kernel<K, RW, false>, 256, 0);
     int per_sm = occ > 0 ? occ : 1;
     if (fp.blend_blocks > 0 && fp.blend_blocks < per_sm) per_sm = fp.blend_blocks;
-    blend_kernel<K, RW><<<n_sms * per_sm, 256, 0, s>>>(fp, fb);
+    if (!(sp.share > 0.0f) || sp.of == nullptr) {
+        blend_kernel<K, RW, false><<<n_sms * per_sm, 256, 0, s>>>(fp, fb);
+        if (mid) cudaEventRecord(mid, s);
+        return 1;
+    }
+    if (occ_split < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_split, blend_split_kernel<K, RW>, 256, 0);
+    int per_sm_split = occ_split > 0 ? occ_split : 1;
+    if (fp.blend_blocks > 0 && fp.blend_blocks < per_sm_split) per_sm_split = fp.blend_blocks;
+    blend_split_kernel<K, RW><<<n_sms * per_sm_split, 256, 0, s>>>(fp, fb, sp);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(n_sms * per_sm);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, blend_kernel<K, RW, true>, fp, fb);
     if (mid) cudaEventRecord(mid, s);
-    return 1;
+    return 2;
 }
 
 template <int K>
-int launch_blend_k(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid) {
+int launch_blend_k(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp, int n_sms, cudaStream_t s,
+                   cudaEvent_t mid) {
     switch (fp.blend_rw) {
-        case 16: return launch_blend_kr<K, 16>(fp, fb, n_sms, s, mid);
-        case 4: return launch_blend_kr<K, 4>(fp, fb, n_sms, s, mid);
-        default: return launch_blend_kr<K, 8>(fp, fb, n_sms, s, mid);
+        case 16: return launch_blend_kr<K, 16>(fp, fb, sp, n_sms, s, mid);
+        case 4: return launch_blend_kr<K, 4>(fp, fb, sp, n_sms, s, mid);
+        default: return launch_blend_kr<K, 8>(fp, fb, sp, n_sms, s, mid);
     }
 }
 
-int launch_blend(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid) {
+int launch_blend(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp, int n_sms, cudaStream_t s,
+                 cudaEvent_t mid) {
     const int K = fp.K;
-    if (K >= 32) return launch_blend_k<32>(fp, fb, n_sms, s, mid);
-    if (K >= 16) return launch_blend_k<16>(fp, fb, n_sms, s, mid);
-    if (K >= 8) return launch_blend_k<8>(fp, fb, n_sms, s, mid);
-    if (K >= 4) return launch_blend_k<4>(fp, fb, n_sms, s, mid);
-    if (K >= 2) return launch_blend_k<2>(fp, fb, n_sms, s, mid);
-    return launch_blend_k<1>(fp, fb, n_sms, s, mid);
+    if (K >= 32) return launch_blend_k<32>(fp, fb, sp, n_sms, s, mid);
+    if (K >= 16) return launch_blend_k<16>(fp, fb, sp, n_sms, s, mid);
+    if (K >= 8) return launch_blend_k<8>(fp, fb, sp, n_sms, s, mid);
+    if (K >= 4) return launch_blend_k<4>(fp, fb, sp, n_sms, s, mid);
+    if (K >= 2) return launch_blend_k<2>(fp, fb, sp, n_sms, s, mid);
+    return launch_blend_k<1>(fp, fb, sp, n_sms, s, mid);
 }
 
 // ------------------------------------------------------------------------------------------

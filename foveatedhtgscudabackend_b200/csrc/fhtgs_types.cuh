@@ -163,7 +163,45 @@ struct FrameBuffers {
 // tiles, the longest lists of each class first (longest-processing-time scheduling).
 constexpr int kCostBuckets = 130;                     // per tile class
 constexpr int kOrderBuckets = 3 * kCostBuckets;       // full-resolution, periphery, quarter
-constexpr int kCounterWords = 4 + 2 * kOrderBuckets;  // counters, histogram, cursors
+// counters[0..2]: next full-resolution / periphery / quarter item of the blend; then the split
+// blend's words; the work-order histogram and cursors follow from kCtrHist.
+constexpr int kCtrSplitNext = 3;      // next split segment of the blend
+constexpr int kCtrSplitSegs = 4;      // segments reserved by the work order
+constexpr int kCtrSplitTiles = 5;     // tiles split
+constexpr int kCtrSplitFallback = 6;  // split tiles blended whole after a record overflow
+constexpr int kCtrSplitRecMax = 7;    // most records a pixel of a later segment produced
+constexpr int kCtrHist = 8;
+constexpr int kCounterWords = kCtrHist + 2 * kOrderBuckets;  // counters, histogram, cursors
+constexpr int kSplitMaxSegments = 8;
+
+// Persistent blend blocks per SM the register allocation has to allow: the K-buffer (2 K
+// registers) dominates for large K.
+__host__ __device__ constexpr int blend_min_blocks(int K) { return K >= 32 ? 2 : K >= 16 ? 3 : 4; }
+
+// Split blend (a tolerance mode, off by default; its own kernel argument so that the other
+// kernels' parameters keep their layout): a full-resolution tile whose list is longer than
+// share x (instances of the frame / blocks) is blended as up to kSplitMaxSegments contiguous
+// segments on different blocks, merged by the last of them.
+struct SplitArgs {
+    float share;           // 0: off
+    int blocks;            // persistent blend blocks of the launch
+    int cap;               // segments the scratch holds
+    int recs;              // records a later segment keeps per pixel
+    int stride;            // bytes of scratch per segment
+    uint32_t* of;          // [V][max_large] per full-resolution item: first segment | S << 28, or ~0
+    uint2* list;           // [cap] per segment: packed item, first segment | S << 28 (~0: unused)
+    uint32_t* ctl;         // [cap] per first segment: segments finished
+    char* scratch;         // [cap][stride] per-pixel state and records
+};
+
+// Split blend scratch of one segment (256 pixels; arrays pixel-fastest):
+//   first segment:  depth[K][256] f32 | color[K][256] u32 | tail[256] float4 | T[256] f32
+//   later segments: n_rec[256] u32 | tail[256] float4 | T[256] f32 | depth[R][256] f32 |
+//                   pm[R][256] float4 (the fragments that entered the segment's K-buffer)
+constexpr int kSplitPx = 256;
+__host__ __device__ constexpr int split_stride_bytes(int K, int R) {
+    return (2 * K + 5 > 6 + 5 * R ? 2 * K + 5 : 6 + 5 * R) * 4 * kSplitPx;
+}
 
 // Launchers exported by each math flavour (fast = -use_fast_math, ieee = default).
 struct KernelSet {
@@ -175,9 +213,12 @@ struct KernelSet {
     int (*create_instances)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);
     int (*sort)(const FrameParams& fp, FrameBuffers& fb, cudaStream_t s);
     int (*ranges)(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s);
-    int (*order)(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s);
+    int (*order)(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp, int n_sms, cudaStream_t s);
     // `mid` (may be null) is recorded right after the blend.
-    int (*blend)(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cudaStream_t s, cudaEvent_t mid);
+    // With the split blend on, the split segments' kernel runs first and the blend of the other
+    // tiles follows it as a programmatic dependent launch.
+    int (*blend)(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp, int n_sms, cudaStream_t s,
+                 cudaEvent_t mid);
     int (*compose)(const FrameParams& fp, const FrameBuffers& fb, cudaStream_t s);
 };
 

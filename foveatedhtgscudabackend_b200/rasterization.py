@@ -427,6 +427,21 @@ class Renderer:
         t = _lib.Tuning(int(blend_warp_width), int(blend_blocks_per_sm), int(sort_items))
         _lib.check(self._libh.fhtgs_context_set_tuning(self.ctx, C.byref(t)))
 
+    def set_blend_split(self, segment_share: float = 0.0, records: int = 0):
+        """Split blend (a tolerance mode; 0 = off, the bit-identical default): full-resolution
+        tiles whose list exceeds segment_share x (instances / blend blocks) are blended as
+        segments merged exactly up to the tail's summation order (fhtgs_context_set_blend_split)."""
+        _lib.check(self._libh.fhtgs_context_set_blend_split(self.ctx, float(segment_share), int(records)))
+
+    def blend_split_stats(self) -> dict:
+        """The last frame's split blend: tiles split, segments, tiles blended whole after a record
+        overflow, and the most records one pixel of a segment produced."""
+        t, g, f, m = C.c_int32(0), C.c_int32(0), C.c_int32(0), C.c_int32(0)
+        _lib.check(self._libh.fhtgs_context_get_blend_split_stats(self.ctx, C.byref(t), C.byref(g), C.byref(f),
+                                                                   C.byref(m)))
+        return dict(split_tiles=int(t.value), segments=int(g.value), whole_fallbacks=int(f.value),
+                    max_records=int(m.value))
+
     def autotune(self, positions, scales, rotations, opacities, sh_0, sh_rest, settings: list[RasterizerSettings],
                  to_chw: bool = True, blur_periphery: bool = False, aaa_mode: bool = False, fast_math: bool = True,
                  repeats: int = 5, view_foveation: list | None = None) -> dict:

@@ -315,6 +315,23 @@ typedef struct fhtgs_tuning {
 } fhtgs_tuning;
 fhtgs_status fhtgs_context_set_tuning(fhtgs_context ctx, const fhtgs_tuning* tuning);
 fhtgs_status fhtgs_context_get_tuning(fhtgs_context ctx, fhtgs_tuning* tuning);
+/* Split blend, a tolerance mode (off by default).  A full-resolution tile's K-buffer walk over its
+ * whole list is the serial critical path of a frame; with the mode on, a tile whose list is
+ * longer than `segment_share` x (the frame's instances / persistent blend blocks) is blended as
+ * up to 8 contiguous segments on different blocks.  Each segment records the fragments that enter
+ * its own K-buffer; the last segment to finish replays them in list order, which reproduces every
+ * K-buffer insertion and eviction of the serial walk (reference blend_cu, inference.cuh:188-240),
+ * so only the float summation order of the tail and of its transmittance changes (images differ
+ * from the bit-identical path by rounding only).  `records` (0 = 8 K + 64) bounds the records a
+ * segment keeps per pixel (20 bytes each); a tile with a pixel over the bound is blended whole,
+ * serially (counted as a fallback).  segment_share: 0 (off) or in [0.05, 8].  Applies from the
+ * next frame. */
+fhtgs_status fhtgs_context_set_blend_split(fhtgs_context ctx, float segment_share, int32_t records);
+/* The last frame's split blend: tiles split, segments blended, tiles blended whole after a record
+ * overflow, and the most records one pixel of a segment produced.  Waits for the context's last
+ * frame. */
+fhtgs_status fhtgs_context_get_blend_split_stats(fhtgs_context ctx, int32_t* split_tiles, int32_t* segments,
+                                                 int32_t* whole_fallbacks, int32_t* max_records);
 /* Autotuner: renders the given frame with each candidate and keeps the fastest.  The blend knobs
  * are chosen first by the blend's CUDA-event time (width x blocks), then sort_items by the
  * sort's; each candidate is timed as the median of `repeats` (1..32) frames after one warm-up
