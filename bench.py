@@ -85,7 +85,7 @@ def parse(argv=None):
     ap.add_argument("--in-flight", type=int, default=2,
                     help="stereo workload: frames in flight, one renderer context and one stream each "
                          "(1 = one frame at a time; the single-frame numbers are reported either way)")
-    ap.add_argument("--blend-split", type=float, default=0.3,
+    ap.add_argument("--blend-split", type=float, default=0.6,
                     help="segment share of the split-blend leg (a tolerance mode); 0 skips the leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")

@@ -144,7 +144,7 @@ struct Layout {
     size_t off_hist, off_dtot, off_ranges, off_map, off_type, off_ltype, off_wf, off_wl, off_wm, off_ctr, off_temp;
     size_t off_order0, off_order1;
     size_t off_ghist, off_look, off_ticket;
-    size_t off_split_of = 0, off_split_list = 0, off_split_ctl = 0, off_split_scratch = 0;
+    size_t off_split_of = 0, off_split_list = 0, off_split_ctl = 0, off_split_scratch = 0, off_split_status = 0;
     std::vector<size_t> temp_offsets;
 };
 
@@ -207,6 +207,7 @@ Layout plan(int V, int64_t N, int nbp, int64_t cap, int key_bytes, int sort_tile
         L.off_split_list = take(8ull * sp.cap);
         L.off_split_ctl = take(4ull * sp.cap);
         L.off_split_scratch = take(static_cast<size_t>(sp.stride) * sp.cap);
+        L.off_split_status = take(sizeof(FrameStatus) * V);
     }
     L.total = o;
     return L;
@@ -420,6 +421,7 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
         sa.list = reinterpret_cast<uint2*>(A + L.off_split_list);
         sa.ctl = reinterpret_cast<uint32_t*>(A + L.off_split_ctl);
         sa.scratch = A + L.off_split_scratch;
+        sa.status = reinterpret_cast<FrameStatus*>(A + L.off_split_status);
     }
 
     std::vector<ViewSetup> setups(V);

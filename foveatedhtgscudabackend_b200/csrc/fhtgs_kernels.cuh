@@ -1316,7 +1316,6 @@ int launch_ranges(const FrameParams& fp, const FrameBuffers& fb, int n_sms, cuda
 // buckets are served heaviest first, so that long serial per-pixel chains start early.
 // ------------------------------------------------------------------------------------------
 constexpr uint32_t kItemLowres = 1u << 23;
-constexpr uint32_t kItemSplit = ~0u;  // a place of a tile the split blend renders (view 255 never exists)
 
 __device__ __forceinline__ int items_of_view(const FrameStatus& st) {
     return static_cast<int>(st.n_fovea_large + st.n_blended_large + st.n_periphery_large + st.n_quarter_large);
@@ -1403,8 +1402,8 @@ __device__ __forceinline__ int items_prefix(const FrameParams& fp, const FrameBu
     return s_total;
 }
 
-// Also decides which full-resolution tiles the split blend splits (their places in the work
-// list hold kItemSplit, and their segments go to the split list) and clears the split tickets.
+// Also decides which full-resolution tiles the split blend splits (they leave the work list,
+// their segments go to the split list) and clears the split tickets.
 __global__ void __launch_bounds__(256) order_hist_kernel(FrameParams fp, FrameBuffers fb, SplitArgs sp) {
     __shared__ int pre[kMaxOrderViews];
     __shared__ uint32_t hist[kOrderBuckets];
@@ -1429,9 +1428,11 @@ __global__ void __launch_bounds__(256) order_hist_kernel(FrameParams fp, FrameBu
                 if (split_reserve(fb, sp, S, seg0)) {
                     tag = seg0 | (S << 28);
                     atomicAdd(&fb.counters[kCtrSplitTiles], 1u);
+                    atomicAdd(&fb.counters[kCtrSplitView + v], 1u);
                 }
             }
             sp.of[static_cast<size_t>(v) * fp.max_large + j] = tag;
+            if (tag != ~0u) continue;
         }
         atomicAdd(&hist[b], 1u);
     }
@@ -1452,6 +1453,12 @@ __global__ void __launch_bounds__(256) order_scatter_kernel(FrameParams fp, Fram
     __shared__ uint32_t s_cnt[kOrderBuckets];
     __shared__ uint32_t s_warp[33];
     const int total = items_prefix(fp, fb, pre);
+    if (sp.status != nullptr && sp.share > 0.0f && blockIdx.x == 0)
+        for (int v = threadIdx.x; v < fp.n_views; v += blockDim.x) {
+            FrameStatus c = fb.status[v];
+            c.n_blended_large -= fb.counters[kCtrSplitView + v];
+            sp.status[v] = c;
+        }
     const uint32_t* gh = fb.counters + kCtrHist;
     uint32_t* cursor = fb.counters + kCtrHist + kOrderBuckets;
     {  // each bucket's first place in descending bucket order: a block scan, two buckets a thread
@@ -1481,7 +1488,7 @@ __global__ void __launch_bounds__(256) order_scatter_kernel(FrameParams fp, Fram
                 if (tag != ~0u) {  // a split tile: its segments go to the split list
                     const uint32_t seg0 = tag & 0x0fffffffu, S = tag >> 28;
                     for (uint32_t k = 0; k < S; ++k) sp.list[seg0 + k] = make_uint2(packed, tag);
-                    packed = kItemSplit;
+                    b = -1;
                 }
             }
             if (b >= 0) local = atomicAdd(&s_cnt[b], 1u);
@@ -2060,8 +2067,8 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_split_kernel(F
 // One persistent kernel blends every tile of every view.  The work list holds the full-resolution
 // tiles, then the periphery tiles, then the quarter tiles, each class heaviest first; blocks take
 // items class by class, each class with its own compiled tile code.
-// SPLIT: launched after blend_split_kernel as its programmatic dependent (its own instantiation,
-// so that the default path's code is not touched by the split blend's).
+// SPLIT: launched after blend_split_kernel as its programmatic dependent, with the status whose
+// full-resolution counts leave out the split tiles (which the work order left out of its list).
 template <int K, int RW, bool SPLIT>
 __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FrameParams fp, FrameBuffers fb) {
     constexpr int NT = 256;
@@ -2086,12 +2093,7 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_kernel(FramePa
         const int g = s_item;
         __syncthreads();
         if (g >= n_full) break;
-        if constexpr (SPLIT) {
-            const uint32_t it = order[g];
-            if (it != kItemSplit) blend_tile<K, RW, 0>(fp, fb, it, sm);  // else the split kernel's
-        } else {
-            blend_tile<K, RW, 0>(fp, fb, order[g], sm);
-        }
+        blend_tile<K, RW, 0>(fp, fb, order[g], sm);
     }
     for (;;) {  // periphery tiles
         if (tid == 0) s_item = static_cast<int>(atomicAdd(&fb.counters[1], 1u));
@@ -2139,7 +2141,9 @@ int launch_blend_kr(const FrameParams& fp, const FrameBuffers& fb, const SplitAr
     cfg.stream = s;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, blend_kernel<K, RW, true>, fp, fb);
+    FrameBuffers rest = fb;  // the other tiles: the status without the split tiles
+    rest.status = sp.status;
+    cudaLaunchKernelEx(&cfg, blend_kernel<K, RW, true>, fp, rest);
     if (mid) cudaEventRecord(mid, s);
     return 2;
 }

@@ -170,7 +170,8 @@ constexpr int kCtrSplitSegs = 4;      // segments reserved by the work order
 constexpr int kCtrSplitTiles = 5;     // tiles split
 constexpr int kCtrSplitFallback = 6;  // split tiles blended whole after a record overflow
 constexpr int kCtrSplitRecMax = 7;    // most records a pixel of a later segment produced
-constexpr int kCtrHist = 8;
+constexpr int kCtrSplitView = 8;      // [256] tiles split per view
+constexpr int kCtrHist = kCtrSplitView + 256;
 constexpr int kCounterWords = kCtrHist + 2 * kOrderBuckets;  // counters, histogram, cursors
 constexpr int kSplitMaxSegments = 8;
 
@@ -192,6 +193,10 @@ struct SplitArgs {
     uint2* list;           // [cap] per segment: packed item, first segment | S << 28 (~0: unused)
     uint32_t* ctl;         // [cap] per first segment: segments finished
     char* scratch;         // [cap][stride] per-pixel state and records
+    // [V] the status the blend of the other tiles reads: the view's, with the split tiles taken
+    // out of n_fovea_large + n_blended_large (that kernel reads only this sum, and n_fovea_large,
+    // which is kept; n_blended_large is adjusted modulo 2^32)
+    FrameStatus* status;
 };
 
 // Split blend scratch of one segment (256 pixels; arrays pixel-fastest):
