@@ -105,6 +105,8 @@ def parse(argv=None):
     ap.add_argument("--slots", type=int, default=2, help="frames in flight (served workload)")
     ap.add_argument("--max-batch", type=int, default=8, help="requests per frame (served workload)")
     ap.add_argument("--no-plain", action="store_true", help="served workload: skip the plain per-request path")
+    ap.add_argument("--served-split", type=float, default=0.0,
+                    help="served workload: the server's split-blend segment share (0 = off, bit-identical)")
     ap.add_argument("--foveation", choices=["reference", "rings", "none"], default="reference",
                     help="reference: the reference's fovea/blend/2x layout (comparable with it); rings: full res "
                          "r < --rings[0], 2x down r < --rings[1], 4x down beyond (NDC); none: all full res")
@@ -810,7 +812,8 @@ def run_served(a, world, rank, local):
     warm = scene.make_served_requests(1.0, 96.0, len(scenes), seed=1000 + rank)
     n_req = len(trace)
 
-    srv = Server(dev, hbm_budget_bytes=150e9, max_in_flight=a.slots, max_batch_requests=a.max_batch)
+    srv = Server(dev, hbm_budget_bytes=150e9, max_in_flight=a.slots, max_batch_requests=a.max_batch,
+                 blend_split=a.served_split)
     ids = [srv.add_scene(*gt, K=a.K, active_sh_bases=active, foveation=a.foveation, rings=tuple(a.rings))
            for gt in scenes]
 
@@ -977,6 +980,7 @@ def run_served(a, world, rank, local):
                    "resolutions_per_eye": "uniform from 1440x1584, 2064x2208", "K": a.K,
                    "head_pose": "sphere r in [4, 8] looking at the origin; gaze N(0, 0.1) NDC",
                    "hbm_budget_gb": 150, "slots": a.slots, "max_batch_requests": a.max_batch,
+                   "blend_split": a.served_split or "off (bit-identical)",
                    "l2": "inputs larger than L2"},
         "latency_ms": {"p50": pct(lat_s, 50), "p99": pct(lat_s, 99), "max": round(max(lat_s), 3)},
         "plain_path": plain,

@@ -85,7 +85,8 @@ class Tuning(C.Structure):
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("device", c_i32), ("max_in_flight", c_i32), ("max_batch_requests", c_i32), ("reserved", c_i32),
+    _fields_ = [("device", c_i32), ("max_in_flight", c_i32), ("max_batch_requests", c_i32),
+                ("blend_split_permille", c_i32),
                 ("hbm_budget_bytes", C.c_int64)]
 
 

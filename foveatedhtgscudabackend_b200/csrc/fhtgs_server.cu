@@ -613,6 +613,8 @@ fhtgs_status fhtgs_server_create(const fhtgs_server_config* config, fhtgs_server
     if (cfg.max_batch_requests < 1 || cfg.max_batch_requests > kMaxBatchRequests)
         return srv_fail(FHTGS_ERR_INVALID_ARGUMENT, "max_batch_requests must be in [1, 64]");
     if (cfg.hbm_budget_bytes < 0) return srv_fail(FHTGS_ERR_INVALID_ARGUMENT, "negative budget");
+    if (cfg.blend_split_permille != 0 && (cfg.blend_split_permille < 50 || cfg.blend_split_permille > 8000))
+        return srv_fail(FHTGS_ERR_INVALID_ARGUMENT, "blend_split_permille must be 0 (off) or in [50, 8000]");
     int n_dev = 0;
     cudaError_t e = cudaGetDeviceCount(&n_dev);
     if (e != cudaSuccess) return srv_fail(FHTGS_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
@@ -641,6 +643,10 @@ fhtgs_status fhtgs_server_create(const fhtgs_server_config* config, fhtgs_server
         sl.server = S;
         st = fhtgs_context_create(cfg.device, &sl.ctx);
         if (st != FHTGS_OK) return bail(st, fhtgs_last_error());
+        if (cfg.blend_split_permille != 0) {
+            st = fhtgs_context_set_blend_split(sl.ctx, static_cast<float>(cfg.blend_split_permille) / 1000.0f, 0);
+            if (st != FHTGS_OK) return bail(st, fhtgs_last_error());
+        }
         if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaMallocHost(&sl.h_cam, sizeof(float) * kCamFloats * kMaxFrameViews) != cudaSuccess ||
             cudaMallocHost(&sl.h_status, sizeof(FrameStatus) * kMaxFrameViews) != cudaSuccess ||

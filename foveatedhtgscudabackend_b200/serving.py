@@ -185,14 +185,14 @@ class Server:
     """Continuous-batching request server on one CUDA device (see the module docstring)."""
 
     def __init__(self, device: int | torch.device | None = None, hbm_budget_bytes: float = 150e9,
-                 max_in_flight: int = 2, max_batch_requests: int = 8):
+                 max_in_flight: int = 2, max_batch_requests: int = 8, blend_split: float = 0.0):
         dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         if dev.type != "cuda":
             raise ValueError("the server needs a CUDA device")
         self.device = torch.device("cuda", dev.index if dev.index is not None else torch.cuda.current_device())
         self._libh = _lib.load()
-        cfg = _lib.ServerConfig(self.device.index, int(max_in_flight), int(max_batch_requests), 0,
-                                int(hbm_budget_bytes))
+        cfg = _lib.ServerConfig(self.device.index, int(max_in_flight), int(max_batch_requests),
+                                int(round(blend_split * 1000)), int(hbm_budget_bytes))
         out = _lib.vp()
         with torch.cuda.device(self.device):
             _lib.check(self._libh.fhtgs_server_create(C.byref(cfg), C.byref(out)))
@@ -316,11 +316,12 @@ class ServerGroup:
     `replica` and `device` set.  Nothing crosses devices per frame."""
 
     def __init__(self, devices: list, hbm_budget_bytes: float = 150e9, max_in_flight: int = 2,
-                 max_batch_requests: int = 8):
+                 max_batch_requests: int = 8, blend_split: float = 0.0):
         self.devices = [torch.device("cuda", torch.device(d).index if not isinstance(d, int) else d) for d in devices]
         self._libh = _lib.load()
         ids = (C.c_int32 * len(self.devices))(*[d.index for d in self.devices])
-        cfg = _lib.ServerConfig(0, int(max_in_flight), int(max_batch_requests), 0, int(hbm_budget_bytes))
+        cfg = _lib.ServerConfig(0, int(max_in_flight), int(max_batch_requests), int(round(blend_split * 1000)),
+                                int(hbm_budget_bytes))
         out = _lib.vp()
         _lib.check(self._libh.fhtgs_server_group_create(ids, len(self.devices), C.byref(cfg), C.byref(out)))
         self.handle = out.value

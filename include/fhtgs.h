@@ -388,14 +388,16 @@ fhtgs_status fhtgs_frame_graph_destroy(fhtgs_frame_graph graph);
  * (counted against the budget, recycled) whose address the completion returns; it stays valid
  * until fhtgs_server_release(ticket).
  * Results: every view is rendered exactly as fhtgs_render_views renders it alone — a request's
- * images do not depend on what else shares its frame. */
+ * images do not depend on what else shares its frame (with blend_split_permille set, up to the
+ * split blend's rounding of the tail sums: which tiles are split depends on the frame). */
 typedef struct fhtgs_server_s* fhtgs_server;
 
 typedef struct {
     int32_t device;
     int32_t max_in_flight;       /* frame slots, 1..8; 0 = 2                                  */
     int32_t max_batch_requests;  /* requests fused into one frame, 1..64; 0 = 8                */
-    int32_t reserved;
+    int32_t blend_split_permille; /* split blend of every frame (fhtgs_context_set_blend_split):
+                                     segment share x 1000, 50..8000; 0 = off                   */
     int64_t hbm_budget_bytes;    /* device memory the server may account for; 0 = 150 GB      */
 } fhtgs_server_config;
 

@@ -148,3 +148,30 @@ def test_split_arguments_are_checked():
             r.set_blend_split(share, rec)
     r.set_blend_split(0.0, 0)
     r.close()
+
+
+def test_server_with_split_blend(stereo):
+    """The request server's frames with the split blend on (config blend_split_permille): every
+    request within rounding of the bit-identical images, alone or fused with others."""
+    from foveatedhtgscudabackend_b200.serving import Server
+    _, gt, (left, right) = stereo
+    exact = render(gt, (left, right))
+    with Server(DEV, max_in_flight=2, max_batch_requests=4, blend_split=0.1) as srv:
+        sid = srv.add_scene(*gt, K=8, active_sh_bases=16)
+        srv.pause()
+        for k in range(4):
+            srv.submit(sid, [left, right], tag=k)
+        srv.resume()
+        got = {}
+        while len(got) < 4:
+            cs = srv.poll(wait_ms=5000)
+            assert cs, "server made no progress"
+            for c in cs:
+                assert c.ok, c.message
+                got[c.tag] = [x.clone() for x in c.images]
+                srv.release(c.ticket)
+    for k in range(4):
+        p, m, n_diff, n_px = compare(exact, got[k])
+        assert m <= 1e-4 and p >= REF_PSNR_DB, f"request {k}: max-abs {m}"
+    with pytest.raises(_lib.FhtgsError):
+        Server(DEV, blend_split=0.01)
