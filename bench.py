@@ -370,6 +370,32 @@ def run_ours(a, world, rank, local):
         step_ms = [fs[k].elapsed_time(fe[k]) for k in range(a.steps)]
         total_ms_max = max_over_ranks(e0.elapsed_time(e1), world)
         value = world * a.steps / (total_ms_max / 1000.0)
+        if split is not None:
+            # the same frames in flight with the split blend on every context
+            for x in rs:
+                x.set_blend_split(a.blend_split, 0)
+            for i in range(n_fl):
+                for _ in range(3):
+                    rs[i].render(*gt, st, to_chw=True, fast_math=True, images=imgs_fl[i], sync=True)
+            barrier(world)
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            for sfl in streams_fl[1:]:
+                sfl.wait_event(e0)
+            for k in range(a.steps):
+                i = k % n_fl
+                with torch.cuda.stream(streams_fl[i]):
+                    rs[i].render(*gt, st, to_chw=True, fast_math=True, images=imgs_fl[i], sync=False)
+            for sfl in streams_fl[1:]:
+                stream.wait_stream(sfl)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            barrier(world)
+            split_ms = max_over_ranks(e0.elapsed_time(e1), world)
+            split["in_flight_value"] = round(world * a.steps / (split_ms / 1000.0), 3)
+            split["frames_in_flight"] = n_fl
+            for x in rs:
+                x.set_blend_split(0.0, 0)
 
     # ---- dominant kernel: full-resolution blend (fovea + blended tiles), per-frame events ----
     stage_avg = {k: statistics.mean(h[k] for h in hist) for k in hist[0]}
