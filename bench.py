@@ -613,6 +613,25 @@ def run_plain(a, world, rank, local):
     launches = r.launch_count() - launches0
     eager_ms, _ = timed(lambda: r.render(*gt, st, images=img, sync=False))
     graph.close()
+    exact = img[0].clone()
+    split = None
+    if a.blend_split > 0:  # the same frame graph with the split blend (tolerance mode)
+        r.set_blend_split(a.blend_split, 0)
+        r.render(*gt, st, images=img, sync=True)
+        sgraph = r.capture(*gt, st, images=img, capacity_headroom=1.1)
+        split_ms, split_per = timed(sgraph.launch)
+        stats = r.blend_split_stats()
+        sgraph.close()
+        r.set_blend_split(0.0, 0)
+        d = (img[0].double() - exact.double()).abs()
+        mse = float((d * d).mean())
+        split = {"segment_share": a.blend_split, "value": round(world * steps / (split_ms / 1000.0), 2),
+                 "unit": "frames/s", "ms_per_step": round(split_ms / steps, 4),
+                 "latency_ms": {"p50": round(float(np.percentile(split_per, 50)), 4),
+                                "p99": round(float(np.percentile(split_per, 99)), 4)}, **stats,
+                 "vs_default_path": {"max_abs": float(d.max()),
+                                     "psnr_db": None if mse == 0 else round(10 * np.log10(1 / mse), 1)},
+                 "note": "tolerance mode: K-buffer decisions exact, tail sums reordered"}
     ref_layout_ms, _ = timed(lambda: _C_benchmarking.benchmark(*gt, *st[0].as_tuple(), True, False, False))
     r.close()
     if rank != 0:
@@ -629,6 +648,7 @@ def run_plain(a, world, rank, local):
         "latency_ms": {"p50": round(float(np.percentile(per, 50)), 4), "p99": round(float(np.percentile(per, 99)), 4)},
         "eager_frames_per_s": round(world * steps / (eager_ms / 1000.0), 2),
         "dropin_reference_layout_frames_per_s": round(world * steps / (ref_layout_ms / 1000.0), 2),
+        "split_blend": split,
         "gpu_launches": int(launches), "clocks": clk,
     }
 
@@ -691,6 +711,23 @@ def run_batched(a, world, rank, local):
     overflow = any(r.frame_info(i)["overflow"] for i in range(len(st)))
     eager_ms, _ = timed(lambda: r.render(*gt, st, images=imgs, sync=False, view_foveation=vf), a.steps)
     graph.close()
+    split = None
+    if a.blend_split > 0:  # the same batch graph with the split blend (tolerance mode)
+        exact = [x.clone() for x in imgs]
+        r.set_blend_split(a.blend_split, 0)
+        r.render(*gt, st, images=imgs, sync=True, view_foveation=vf)
+        sgraph = r.capture(*gt, st, images=imgs, capacity_headroom=1.1, view_foveation=vf)
+        for _ in range(max(a.warmup, 0)):
+            sgraph.launch()
+        split_ms, _ = timed(sgraph.launch, a.steps)
+        stats = r.blend_split_stats()
+        sgraph.close()
+        r.set_blend_split(0.0, 0)
+        dmax = max(float((x.double() - y.double()).abs().max()) for x, y in zip(imgs, exact))
+        split = {"segment_share": a.blend_split, "value": round(world * a.steps * len(st) / (split_ms / 1000.0), 2),
+                 "unit": "views/s", "ms_per_step": round(split_ms / a.steps, 3), **stats,
+                 "vs_default_path_max_abs": dmax,
+                 "note": "tolerance mode: K-buffer decisions exact, tail sums reordered"}
     # plain per-request path: one blocking call per view, each with its own foveation
     rp = F.Renderer(dev)
     plain_steps = max(1, min(a.steps, 3))
@@ -723,7 +760,7 @@ def run_batched(a, world, rank, local):
         "plain_per_view_views_per_s": round(world * plain_steps * nv / (plain_ms / 1000.0), 2),
         "plain_per_view_api": "Renderer.render(sync=True), one blocking call per view (the drop-in has only the reference's foveation)",
         "view_regions": rings,
-        "tuning": tuning, "overflow": overflow, "gpu_launches": int(launches), "clocks": clk,
+        "tuning": tuning, "overflow": overflow, "split_blend": split, "gpu_launches": int(launches), "clocks": clk,
     }
 
 
