@@ -615,8 +615,10 @@ def run_plain(a, world, rank, local):
     graph.close()
     exact = img[0].clone()
     split = None
-    if a.blend_split > 0:  # the same frame graph with the split blend (tolerance mode)
-        r.set_blend_split(a.blend_split, 0)
+    split = split_exact = None
+
+    def split_graph(exact_mode: bool) -> dict:
+        r.set_blend_split(a.blend_split, 0, exact=exact_mode)
         r.render(*gt, st, images=img, sync=True)
         sgraph = r.capture(*gt, st, images=img, capacity_headroom=1.1)
         split_ms, split_per = timed(sgraph.launch)
@@ -625,13 +627,17 @@ def run_plain(a, world, rank, local):
         r.set_blend_split(0.0, 0)
         d = (img[0].double() - exact.double()).abs()
         mse = float((d * d).mean())
-        split = {"segment_share": a.blend_split, "value": round(world * steps / (split_ms / 1000.0), 2),
-                 "unit": "frames/s", "ms_per_step": round(split_ms / steps, 4),
-                 "latency_ms": {"p50": round(float(np.percentile(split_per, 50)), 4),
-                                "p99": round(float(np.percentile(split_per, 99)), 4)}, **stats,
-                 "vs_default_path": {"max_abs": float(d.max()),
-                                     "psnr_db": None if mse == 0 else round(10 * np.log10(1 / mse), 1)},
-                 "note": "tolerance mode: K-buffer decisions exact, tail sums reordered"}
+        return {"segment_share": a.blend_split, "value": round(world * steps / (split_ms / 1000.0), 2),
+                "unit": "frames/s", "ms_per_step": round(split_ms / steps, 4),
+                "latency_ms": {"p50": round(float(np.percentile(split_per, 50)), 4),
+                               "p99": round(float(np.percentile(split_per, 99)), 4)}, **stats,
+                "vs_default_path": {"max_abs": float(d.max()),
+                                    "psnr_db": None if mse == 0 else round(10 * np.log10(1 / mse), 1)},
+                "note": "fragment logs replayed in list order: bit-identical" if exact_mode else
+                        "tolerance mode: K-buffer decisions exact, tail sums reordered"}
+    if a.blend_split > 0:  # the same frame graph with the split blend, both modes
+        split = split_graph(False)
+        split_exact = split_graph(True)
     ref_layout_ms, _ = timed(lambda: _C_benchmarking.benchmark(*gt, *st[0].as_tuple(), True, False, False))
     r.close()
     if rank != 0:
@@ -649,6 +655,7 @@ def run_plain(a, world, rank, local):
         "eager_frames_per_s": round(world * steps / (eager_ms / 1000.0), 2),
         "dropin_reference_layout_frames_per_s": round(world * steps / (ref_layout_ms / 1000.0), 2),
         "split_blend": split,
+        "split_blend_exact": split_exact,
         "gpu_launches": int(launches), "clocks": clk,
     }
 

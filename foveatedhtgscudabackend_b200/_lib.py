@@ -148,6 +148,7 @@ SIGNATURES = {
     "fhtgs_context_set_tuning": ([vp, C.POINTER(Tuning)], c_i32),
     "fhtgs_context_get_tuning": ([vp, C.POINTER(Tuning)], c_i32),
     "fhtgs_context_set_blend_split": ([vp, c_f, c_i32], c_i32),
+    "fhtgs_context_set_blend_split_exact": ([vp, c_i32, C.c_int64], c_i32),
     "fhtgs_context_get_blend_split_stats": ([vp] + [C.POINTER(c_i32)] * 4, c_i32),
     "fhtgs_autotune": ([vp, C.POINTER(Primitives), C.POINTER(View), c_i32, C.POINTER(Settings), c_i32,
                         C.POINTER(Tuning), C.POINTER(C.c_float), vp], c_i32),

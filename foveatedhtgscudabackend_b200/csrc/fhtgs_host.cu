@@ -109,6 +109,8 @@ struct fhtgs_context_s {
     bool capturing = false;           // a frame graph is being captured: no profiling events
     fhtgs_tuning tuning{8, 0, kSortItems};
     float split_share = 0.0f;     // split blend: 0 = off (bit-identical blend)
+    int split_exact = 0;          // 1: the exact split (fragment logs, bit-identical images)
+    int64_t split_pool = 0;       // bytes of the exact split's fragment log
     bool split_active = false;    // the last frame ran the split blend
     int split_recs = 0;           // records per pixel of a later segment; 0 = 8 K + 64
     int64_t cap = 0;              // instance slots per view
@@ -145,24 +147,31 @@ struct Layout {
     size_t off_order0, off_order1;
     size_t off_ghist, off_look, off_ticket;
     size_t off_split_of = 0, off_split_list = 0, off_split_ctl = 0, off_split_scratch = 0, off_split_status = 0;
+    size_t off_split_units = 0, off_split_pool = 0;
     std::vector<size_t> temp_offsets;
 };
 
 // Split blend sizes of a frame (all zero when the mode is off).
 struct SplitPlan {
     float share = 0.0f;
-    int blocks = 0, cap = 0, recs = 0, stride = 0;
+    int blocks = 0, cap = 0, recs = 0, stride = 0, exact = 0;
+    uint32_t pool_units = 0;
 };
 
-SplitPlan split_plan(float share, int recs, int K, int blend_blocks_per_sm, int n_sms, int V, int max_large) {
+constexpr int64_t kSplitPoolDefault = int64_t(8) << 30;  // exact split: fragment log bytes
+
+SplitPlan split_plan(float share, int recs, int exact, int64_t pool, int K, int blend_blocks_per_sm, int n_sms, int V,
+                     int max_large) {
     SplitPlan sp;
     if (!(share > 0.0f)) return sp;
+    sp.exact = exact;
+    if (exact) sp.pool_units = static_cast<uint32_t>((pool > 0 ? pool : kSplitPoolDefault) / 256);
     const int Ki = K >= 32 ? 32 : K >= 16 ? 16 : K >= 8 ? 8 : K >= 4 ? 4 : K >= 2 ? 2 : 1;  // the blend's K
     const int per_sm = blend_blocks_per_sm > 0 ? std::min(blend_blocks_per_sm, blend_min_blocks(Ki)) : blend_min_blocks(Ki);
     sp.share = share;
     sp.blocks = n_sms * per_sm;
-    sp.recs = recs > 0 ? recs : 8 * Ki + 64;  // 20 bytes each
-    sp.stride = split_stride_bytes(Ki, sp.recs);
+    sp.recs = exact ? 0 : recs > 0 ? recs : 8 * Ki + 64;  // 20 bytes each
+    sp.stride = exact ? 0 : split_stride_bytes(Ki, sp.recs);
     // Segments of about the threshold's length cover at most instances / threshold = blocks /
     // share list entries; tiles whose reservation does not fit are blended whole.
     const int64_t bound = static_cast<int64_t>(std::ceil(sp.blocks / static_cast<double>(share))) + 8 * kSplitMaxSegments;
@@ -208,6 +217,8 @@ Layout plan(int V, int64_t N, int nbp, int64_t cap, int key_bytes, int sort_tile
         L.off_split_ctl = take(4ull * sp.cap);
         L.off_split_scratch = take(static_cast<size_t>(sp.stride) * sp.cap);
         L.off_split_status = take(sizeof(FrameStatus) * V);
+        L.off_split_units = take(4ull * sp.cap);
+        L.off_split_pool = take(256ull * sp.pool_units);
     }
     L.total = o;
     return L;
@@ -317,8 +328,8 @@ FramePlan frame_plan(fhtgs_context ctx, const fhtgs_primitives* prims, const fht
     std::vector<int64_t> temp_floats(V, 0);
     if (s->blur_periphery)
         for (int i = 0; i < V; ++i) temp_floats[i] = 3ll * views[i].width * views[i].height;
-    P.split = split_plan(ctx->split_share, ctx->split_recs, s->K, ctx->tuning.blend_blocks_per_sm, ctx->n_sms, V,
-                         P.max_large);
+    P.split = split_plan(ctx->split_share, ctx->split_recs, ctx->split_exact, ctx->split_pool, s->K,
+                         ctx->tuning.blend_blocks_per_sm, ctx->n_sms, V, P.max_large);
     P.L = plan(V, N, P.nbp, cap, P.key_u32 ? 4 : 2, P.sort_tiles, P.max_tiles, P.max_large, temp_floats, P.split);
     return P;
 }
@@ -422,6 +433,10 @@ fhtgs_status render_impl(fhtgs_context ctx, const fhtgs_primitives* prims, const
         sa.ctl = reinterpret_cast<uint32_t*>(A + L.off_split_ctl);
         sa.scratch = A + L.off_split_scratch;
         sa.status = reinterpret_cast<FrameStatus*>(A + L.off_split_status);
+        sa.exact = P.split.exact;
+        sa.pool_units = P.split.pool_units;
+        sa.seg_unit = reinterpret_cast<uint32_t*>(A + L.off_split_units);
+        sa.pool = A + L.off_split_pool;
     }
 
     std::vector<ViewSetup> setups(V);
@@ -677,8 +692,8 @@ fhtgs_status fhtgs_context_reserve(fhtgs_context ctx, int32_t n_primitives, int3
     std::vector<int64_t> temp(n_views, 3ll * max_width * max_height);
     Layout L = plan(n_views, n_primitives, nbp, ctx->cap, end_bit_of(n_tiles + 1) > 16 ? 4 : 2,
                     sort_tiles_for(ctx->cap, kSortItemsMin), n_tiles, n_large, temp,
-                    split_plan(ctx->split_share, ctx->split_recs, 32, ctx->tuning.blend_blocks_per_sm, ctx->n_sms,
-                               n_views, n_large));
+                    split_plan(ctx->split_share, ctx->split_recs, ctx->split_exact, ctx->split_pool, 32,
+                               ctx->tuning.blend_blocks_per_sm, ctx->n_sms, n_views, n_large));
     return ensure_arena(ctx, L.total);
 }
 
@@ -865,6 +880,16 @@ fhtgs_status fhtgs_context_set_blend_split(fhtgs_context ctx, float segment_shar
     if (records < 0 || records > 256) return fail(FHTGS_ERR_INVALID_ARGUMENT, "records must be in [0, 256]");
     ctx->split_share = segment_share;
     ctx->split_recs = records;
+    return FHTGS_OK;
+}
+
+fhtgs_status fhtgs_context_set_blend_split_exact(fhtgs_context ctx, int32_t exact, int64_t log_bytes) {
+    if (!ctx) return fail(FHTGS_ERR_INVALID_ARGUMENT, "null argument");
+    if (exact != 0 && exact != 1) return fail(FHTGS_ERR_INVALID_ARGUMENT, "exact must be 0 or 1");
+    if (log_bytes != 0 && (log_bytes < (int64_t(1) << 20) || log_bytes > (int64_t(64) << 30)))
+        return fail(FHTGS_ERR_INVALID_ARGUMENT, "log_bytes must be 0 (8 GiB) or in [1 MiB, 64 GiB]");
+    ctx->split_exact = exact;
+    ctx->split_pool = log_bytes;
     return FHTGS_OK;
 }
 

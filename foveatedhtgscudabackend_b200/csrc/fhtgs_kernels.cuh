@@ -1376,12 +1376,25 @@ __device__ __forceinline__ uint32_t split_threshold(const FrameParams& fp, const
     return t < 256.0 ? 256u : t > 4.0e9 ? 4000000000u : static_cast<uint32_t>(t);
 }
 
-// Reserves S consecutive segments for a split tile (one atomic).  A reservation that does not
-// fit the scratch fails and marks the slots it reached below the capacity unused.
-__device__ __forceinline__ bool split_reserve(const FrameBuffers& fb, const SplitArgs& sp, uint32_t S, uint32_t& seg0) {
+// Reserves S consecutive segments for a split tile of `len` list entries (one atomic; in the
+// exact mode a second one for the segments' fragment logs).  A reservation that does not fit
+// fails and marks the segment slots it reached below the capacity unused.
+__device__ __forceinline__ bool split_reserve(const FrameBuffers& fb, const SplitArgs& sp, uint32_t S, uint32_t len,
+                                              uint32_t& seg0) {
     seg0 = atomicAdd(&fb.counters[kCtrSplitSegs], S);
-    if (seg0 + S <= static_cast<uint32_t>(sp.cap)) return true;
-    for (uint32_t k = seg0; k < static_cast<uint32_t>(sp.cap); ++k) sp.list[k] = make_uint2(0u, ~0u);
+    bool ok = seg0 + S <= static_cast<uint32_t>(sp.cap);
+    if (ok && sp.exact) {
+        const uint32_t units = split_log_units((len + S - 1) / S);
+        const unsigned long long want = static_cast<unsigned long long>(units) * S;
+        // a 64-bit count (words kCtrSplitPool, +1), so that failed reservations cannot wrap it
+        unsigned long long* pool_used = reinterpret_cast<unsigned long long*>(&fb.counters[kCtrSplitPool]);
+        const unsigned long long u0 = want <= sp.pool_units ? atomicAdd(pool_used, want) : sp.pool_units;
+        ok = want <= sp.pool_units && u0 + want <= sp.pool_units;
+        if (ok)
+            for (uint32_t k = 0; k < S; ++k) sp.seg_unit[seg0 + k] = static_cast<uint32_t>(u0) + k * units;
+    }
+    if (ok) return true;
+    for (uint32_t k = seg0; k < seg0 + S && k < static_cast<uint32_t>(sp.cap); ++k) sp.list[k] = make_uint2(0u, ~0u);
     return false;
 }
 
@@ -1425,7 +1438,7 @@ __global__ void __launch_bounds__(256) order_hist_kernel(FrameParams fp, FrameBu
             uint32_t tag = ~0u, seg0;
             if (len > split_len) {
                 const uint32_t S = min(static_cast<uint32_t>(kSplitMaxSegments), (len + split_len - 1) / split_len);
-                if (split_reserve(fb, sp, S, seg0)) {
+                if (split_reserve(fb, sp, S, len, seg0)) {
                     tag = seg0 | (S << 28);
                     atomicAdd(&fb.counters[kCtrSplitTiles], 1u);
                     atomicAdd(&fb.counters[kCtrSplitView + v], 1u);
@@ -1784,7 +1797,9 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
     }
     const uint32_t* vals = fb.vals[fb.final_buf] + static_cast<size_t>(v) * fp.cap;
     const float4* rec = fb.rec + 4 * static_cast<size_t>(v) * fp.n_prims;
-    uint32_t n_rec = 0;  // SEG mode 2: fragments that entered the K-buffer
+    uint32_t n_rec = 0;     // SEG mode 2: fragments that entered the K-buffer
+    uint32_t n_logged = 0;  // SEG mode 3: steps of this warp logged so far
+    constexpr bool log_mode = SEG == 3;  // the exact split's segment: log the fragments only
 
     float tail_T = 1.0f;
     float4 tail = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -1835,9 +1850,19 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
             const bool hit = j < n_batch && ((sm.mask[j] >> warp) & 1u);
             const uint32_t b = __ballot_sync(0xffffffffu, hit);
             if (hit) sm.list[warp][n_mine + __popc(b & lanemask_lt)] = static_cast<uint8_t>(j);
+            if constexpr (log_mode) {
+                if (hit)  // each step's Gaussian colour and opacity
+                    reinterpret_cast<float4*>(sw.scratch + 256u * split_log_pos_unit())
+                        [static_cast<uint32_t>(warp) * sw.recs + n_logged + n_mine + __popc(b & lanemask_lt)] = sm.rgba[j];
+            }
             n_mine += __popc(b);
         }
         __syncwarp();
+        uint32_t step0 = 0;
+        if constexpr (SEG != 0) {
+            step0 = n_logged;
+            n_logged += static_cast<uint32_t>(n_mine);
+        }
         if (!inside) continue;
         for (int t = 0; t < n_mine; ++t) {
             const int j = sm.list[warp][t];
@@ -1864,11 +1889,13 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
             // evaluated when some lane of the warp has such a fragment (a warp-uniform branch,
             // so that warps whose fragments are all faint skip it without reconvergence work)
             const bool cand = frag && alpha >= kMinAlphaCore;
+            float logged_depth = 0.0f;
             if (__any_sync(__activemask(), cand)) {
                 const float3 ep = cross(d, m) * den_rcp;
                 const float depth = dot(xyz(VPMT4), ep) + VPMT4.w;
-                if (cand && depth < core[K - 1].depth) {
-                    if constexpr (SEG != 0) {
+                if constexpr (log_mode) logged_depth = depth;
+                if (cand && depth < core[K - 1].depth && !log_mode) {
+                    if constexpr (SEG == 1) {
                         if (sw.mode == 2) {  // recorded; the merge decides what it does
                             if (n_rec < static_cast<uint32_t>(sw.recs)) {
                                 reinterpret_cast<float*>(sw.scratch + 6 * 4 * NT)[n_rec * NT + tid] = depth;
@@ -1889,9 +1916,17 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
                         }
                     }
                     pm = unpack_rgba(f.color);
-                    if constexpr (SEG != 0) {
+                    if constexpr (SEG == 1) {
                         if (sw.mode == 2) pm = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // adds nothing below
                     }
+                }
+            }
+            if constexpr (log_mode) {
+                {  // the pair's alpha (-1: no fragment) and depth, for the replay
+                    reinterpret_cast<float2*>(sw.scratch + 256u * split_log_frag_unit(sw.recs))
+                        [(static_cast<uint32_t>(warp) * sw.recs + step0 + t) * 32u + lane] =
+                        make_float2(frag ? alpha : -1.0f, logged_depth);
+                    continue;
                 }
             }
             if (frag) {
@@ -1901,7 +1936,7 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
             }
         }
     }
-    if constexpr (SEG != 0) {
+    if constexpr (SEG == 1) {
         if (sw.mode == 1) {
             float* cd = reinterpret_cast<float*>(sw.scratch);
             uint32_t* cc = reinterpret_cast<uint32_t*>(sw.scratch + K * 4 * NT);
@@ -1920,6 +1955,10 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
             reinterpret_cast<float*>(sw.scratch + 5 * 4 * NT)[tid] = tail_T;
             return;
         }
+    }
+    if constexpr (log_mode) {
+        if (lane == 0) reinterpret_cast<uint32_t*>(sw.scratch)[warp] = n_logged;
+        return;
     }
     if (inside) {
         float3 rgb = make_float3(0.0f, 0.0f, 0.0f);
@@ -1947,24 +1986,93 @@ __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuf
     }
 }
 
-// One segment of a split full-resolution tile (split list entry g).  The last of the tile's
-// segments to finish merges them: per pixel it starts from the first segment's K-buffer and
-// tail, and replays every later segment's records in list order with the K-buffer's own
-// insertion rule.  A fragment that never entered its segment's (initially empty) K-buffer can
-// never enter the true one, whose K-th depth is never larger, so the replay reproduces every
-// insertion and eviction of the serial walk exactly; only the tail sums and the transmittance
-// products are combined in a different order.  If some pixel recorded more fragments than the
-// scratch holds, the merging block blends the whole tile serially instead.
+// Exact split: the merge.  Each pixel replays, segment by segment and step by step, the
+// fragments its warp evaluated, with the walk's own K-buffer insertion and tail accumulation, so
+// the operations and their order are those of the serial walk over the whole list.
 template <int K, int RW>
-__device__ __forceinline__ void blend_split_segment(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp,
-                                                    uint32_t g, const BlendSmem& sm) {
+__device__ __forceinline__ void split_replay(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp,
+                                             uint32_t packed, uint32_t seg0, uint32_t S, uint32_t log_stride) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int v = static_cast<int>(packed >> 24);
+    const int item = static_cast<int>(packed & (kItemLowres - 1u));
+    const ViewParams& vp = fb.views[v];
+    const uint32_t lt = fb.work_full[static_cast<size_t>(v) * fp.max_large + item];
+    const bool is_fovea = static_cast<uint32_t>(item) < fb.status[v].n_fovea_large;
+    constexpr int rw_bits = RW == 4 ? 2 : RW == 8 ? 3 : 4;
+    constexpr int rw = 1 << rw_bits, rh = 32 >> rw_bits;
+    constexpr int wx_bits = 4 - rw_bits;
+    const int px_i = static_cast<int>(lt % static_cast<uint32_t>(vp.glw)) * kTileLarge + (warp & ((1 << wx_bits) - 1)) * rw + (lane & (rw - 1));
+    const int py_i = static_cast<int>(lt / static_cast<uint32_t>(vp.glw)) * kTileLarge + (warp >> wx_bits) * rh + (lane >> rw_bits);
+    if (px_i >= vp.width || py_i >= vp.height) return;
+    float tail_T = 1.0f;
+    float4 tail = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    Frag core[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) { core[k].depth = 3.402823466e+38f; core[k].color = 0u; }
+    constexpr uint32_t kChunk = 4;  // steps whose log entries are loaded before any is replayed
+    for (uint32_t k = 0; k < S; ++k) {
+        const char* b = sp.pool + 256ull * sp.seg_unit[seg0 + k];
+        const uint32_t n = __ldcg(reinterpret_cast<const uint32_t*>(b) + warp);
+        const float4* col = reinterpret_cast<const float4*>(b + 256u * split_log_pos_unit()) +
+                            static_cast<size_t>(warp) * log_stride;
+        const float2* fr = reinterpret_cast<const float2*>(b + 256u * split_log_frag_unit(log_stride)) +
+                           static_cast<size_t>(warp) * log_stride * 32u + lane;
+        for (uint32_t t0 = 0; t0 < n; t0 += kChunk) {
+            float2 ads[kChunk];
+            float4 cs[kChunk];
+#pragma unroll
+            for (uint32_t i = 0; i < kChunk; ++i) {
+                const bool ok = t0 + i < n;
+                ads[i] = ok ? __ldcg(fr + (t0 + i) * 32u) : make_float2(-1.0f, 0.0f);
+                cs[i] = ok ? __ldcg(col + t0 + i) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+#pragma unroll
+            for (uint32_t i = 0; i < kChunk; ++i) {
+            const float2 ad = ads[i];
+            if (ad.x < 0.0f) continue;  // not a fragment
+            const float alpha = ad.x;
+            const float4 c = cs[i];
+            float4 pm = make_float4(c.x * alpha, c.y * alpha, c.z * alpha, alpha);
+            const bool cand = alpha >= kMinAlphaCore;
+            if (cand && ad.y < core[K - 1].depth) {
+                Frag f;
+                f.depth = ad.y;
+                f.color = pack_rgba(pm);
+#pragma unroll
+                for (int q = 0; q < K; ++q) {
+                    if (f.depth < core[q].depth) {
+                        const Frag tf = core[q];
+                        core[q] = f;
+                        f = tf;
+                    }
+                }
+                pm = unpack_rgba(f.color);
+            }
+            const float pt = 1.0f - pm.w;
+            tail += pm;
+            tail_T *= pt;
+            }
+        }
+    }
+    blend_resolve<K>(fp, vp, core, tail, tail_T, __uint2float_rn(static_cast<uint32_t>(px_i)),
+                     __uint2float_rn(static_cast<uint32_t>(py_i)), is_fovea ? vp.image : vp.work, px_i, py_i);
+}
+
+// The records mode's segment and merge.  The last of the tile's segments to finish merges them:
+// per pixel it starts from the first segment's K-buffer and tail, and replays every later
+// segment's records in list order with the K-buffer's own insertion rule.  A fragment that never
+// entered its segment's (initially empty) K-buffer can never enter the true one, whose K-th
+// depth is never larger, so the replay reproduces every insertion and eviction of the serial
+// walk exactly; only the tail sums and the transmittance products are combined in a different
+// order.  If some pixel recorded more fragments than the scratch holds, the merging block blends
+// the whole tile serially instead.
+template <int K, int RW>
+__device__ __forceinline__ void blend_split_records(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp,
+                                                    uint32_t g, const BlendSmem& sm, uint32_t packed, uint32_t seg0,
+                                                    uint32_t S, uint32_t s, size_t stride) {
     constexpr int NT = 256;
     __shared__ int s_last;
     const int tid = threadIdx.x;
-    const uint2 e = sp.list[g];
-    if (e.y == ~0u) return;  // a slot of a reservation that did not fit
-    const uint32_t packed = e.x, seg0 = e.y & 0x0fffffffu, S = e.y >> 28, s = g - seg0;
-    const size_t stride = static_cast<size_t>(sp.stride);
     blend_tile<K, RW, 0, 1>(fp, fb, packed, sm, SegWalk{s, S, s == 0 ? 1 : 2, sp.recs, sp.scratch + g * stride});
     __threadfence();
     __syncthreads();
@@ -2039,10 +2147,42 @@ __device__ __forceinline__ void blend_split_segment(const FrameParams& fp, const
                      __uint2float_rn(static_cast<uint32_t>(py_i)), is_fovea ? vp.image : vp.work, px_i, py_i);
 }
 
+// One segment of a split full-resolution tile (split list entry g): the exact split's log and
+// replay (EXACT), or the records mode's segment and merge.
+template <int K, int RW, bool EXACT>
+__device__ __forceinline__ void blend_split_segment(const FrameParams& fp, const FrameBuffers& fb, const SplitArgs& sp,
+                                                    uint32_t g, const BlendSmem& sm) {
+    __shared__ int s_last;
+    const int tid = threadIdx.x;
+    const uint2 e = sp.list[g];
+    if (e.y == ~0u) return;  // a slot of a reservation that did not fit
+    const uint32_t packed = e.x, seg0 = e.y & 0x0fffffffu, S = e.y >> 28, s = g - seg0;
+    const size_t stride = static_cast<size_t>(sp.stride);
+    if constexpr (EXACT) {
+        const int v = static_cast<int>(packed >> 24);
+        const uint32_t lt = fb.work_full[static_cast<size_t>(v) * fp.max_large + (packed & (kItemLowres - 1u))];
+        const uint2 r = fb.ranges[static_cast<size_t>(v) * fp.max_large + lt];
+        const uint32_t len = r.y > r.x ? r.y - r.x : 0u;
+        const uint32_t log_stride = (len + S - 1u) / S;  // steps a warp of one segment can take
+        blend_tile<K, RW, 0, 3>(fp, fb, packed, sm,
+                                SegWalk{s, S, 3, static_cast<int>(log_stride), sp.pool + 256ull * sp.seg_unit[g]});
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) s_last = atomicAdd(&sp.ctl[seg0], 1u) == S - 1u;
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+        split_replay<K, RW>(fp, fb, sp, packed, seg0, S, log_stride);
+        return;
+    } else {
+        blend_split_records<K, RW>(fp, fb, sp, g, sm, packed, seg0, S, s, stride);
+    }
+}
+
 // The split segments of a frame, longest lists first, on persistent blocks; it lets the blend of
 // the other tiles (launched after it as its programmatic dependent) start at once, so that
 // those blocks take the SMs as this kernel's blocks run out of segments.
-template <int K, int RW>
+template <int K, int RW, bool EXACT>
 __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_split_kernel(FrameParams fp, FrameBuffers fb,
                                                                               SplitArgs sp) {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
@@ -2060,7 +2200,7 @@ __global__ void __launch_bounds__(256, blend_min_blocks(K)) blend_split_kernel(F
         const uint32_t g = static_cast<uint32_t>(s_item);
         __syncthreads();
         if (g >= n_seg) break;
-        blend_split_segment<K, RW>(fp, fb, sp, g, sm);
+        blend_split_segment<K, RW, EXACT>(fp, fb, sp, g, sm);
     }
 }
 
@@ -2127,10 +2267,11 @@ int launch_blend_kr(const FrameParams& fp, const FrameBuffers& fb, const SplitAr
         if (mid) cudaEventRecord(mid, s);
         return 1;
     }
-    if (occ_split < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_split, blend_split_kernel<K, RW>, 256, 0);
+    if (occ_split < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_split, blend_split_kernel<K, RW, false>, 256, 0);
     int per_sm_split = occ_split > 0 ? occ_split : 1;
     if (fp.blend_blocks > 0 && fp.blend_blocks < per_sm_split) per_sm_split = fp.blend_blocks;
-    blend_split_kernel<K, RW><<<n_sms * per_sm_split, 256, 0, s>>>(fp, fb, sp);
+    if (sp.exact) blend_split_kernel<K, RW, true><<<n_sms * per_sm_split, 256, 0, s>>>(fp, fb, sp);
+    else blend_split_kernel<K, RW, false><<<n_sms * per_sm_split, 256, 0, s>>>(fp, fb, sp);
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;

@@ -170,7 +170,9 @@ constexpr int kCtrSplitSegs = 4;      // segments reserved by the work order
 constexpr int kCtrSplitTiles = 5;     // tiles split
 constexpr int kCtrSplitFallback = 6;  // split tiles blended whole after a record overflow
 constexpr int kCtrSplitRecMax = 7;    // most records a pixel of a later segment produced
-constexpr int kCtrSplitView = 8;      // [256] tiles split per view
+constexpr int kCtrSplitPool = 8;      // exact mode: 256-byte units of the fragment log reserved
+                                      // (64-bit: words 8 and 9)
+constexpr int kCtrSplitView = 16;     // [256] tiles split per view
 constexpr int kCtrHist = kCtrSplitView + 256;
 constexpr int kCounterWords = kCtrHist + 2 * kOrderBuckets;  // counters, histogram, cursors
 constexpr int kSplitMaxSegments = 8;
@@ -197,7 +199,21 @@ struct SplitArgs {
     // out of n_fovea_large + n_blended_large (that kernel reads only this sum, and n_fovea_large,
     // which is kept; n_blended_large is adjusted modulo 2^32)
     FrameStatus* status;
+    // Exact mode (bit-identical images): every segment logs, per pixel and in list order, the
+    // alpha and depth of each Gaussian its warp evaluates; the last segment of a tile replays the
+    // whole log with the walk's own K-buffer and tail steps.
+    int exact;
+    uint32_t pool_units;   // 256-byte units of the fragment log
+    char* pool;
+    uint32_t* seg_unit;    // [cap] first unit of each segment's log
 };
+
+// Exact split: a segment's log, for a segment of at most `stride` list entries (each warp walks
+// at most that many steps): n_steps[8] u32 | rgba[8][stride] float4 (each step's Gaussian colour
+// and opacity) | frag[8][stride][32] float2 (alpha, or -1 where the pair is no fragment; depth).
+__host__ __device__ inline uint32_t split_log_pos_unit() { return 1u; }
+__host__ __device__ inline uint32_t split_log_frag_unit(uint32_t stride) { return 1u + (stride + 1u) / 2u; }
+__host__ __device__ inline uint32_t split_log_units(uint32_t stride) { return split_log_frag_unit(stride) + 8u * stride; }
 
 // Split blend scratch of one segment (256 pixels; arrays pixel-fastest):
 //   first segment:  depth[K][256] f32 | color[K][256] u32 | tail[256] float4 | T[256] f32

@@ -427,11 +427,15 @@ class Renderer:
         t = _lib.Tuning(int(blend_warp_width), int(blend_blocks_per_sm), int(sort_items))
         _lib.check(self._libh.fhtgs_context_set_tuning(self.ctx, C.byref(t)))
 
-    def set_blend_split(self, segment_share: float = 0.0, records: int = 0):
-        """Split blend (a tolerance mode; 0 = off, the bit-identical default): full-resolution
-        tiles whose list exceeds segment_share x (instances / blend blocks) are blended as
-        segments merged exactly up to the tail's summation order (fhtgs_context_set_blend_split)."""
+    def set_blend_split(self, segment_share: float = 0.0, records: int = 0, exact: bool = False,
+                        log_bytes: int = 0):
+        """Split blend (0 = off, the default): full-resolution tiles whose list exceeds
+        segment_share x (instances / blend blocks) are blended as segments on several blocks.
+        exact=False: merged exactly up to the tail's summation order (fhtgs_context_set_blend_split);
+        exact=True: the segments log their fragments and the merge replays them in order, images
+        bit-identical to the default path (fhtgs_context_set_blend_split_exact)."""
         _lib.check(self._libh.fhtgs_context_set_blend_split(self.ctx, float(segment_share), int(records)))
+        _lib.check(self._libh.fhtgs_context_set_blend_split_exact(self.ctx, 1 if exact else 0, int(log_bytes)))
 
     def blend_split_stats(self) -> dict:
         """The last frame's split blend: tiles split, segments, tiles blended whole after a record

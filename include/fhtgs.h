@@ -327,6 +327,14 @@ fhtgs_status fhtgs_context_get_tuning(fhtgs_context ctx, fhtgs_tuning* tuning);
  * serially (counted as a fallback).  segment_share: 0 (off) or in [0.05, 8].  Applies from the
  * next frame. */
 fhtgs_status fhtgs_context_set_blend_split(fhtgs_context ctx, float segment_share, int32_t records);
+/* The exact split blend (exact = 1; 0 returns to the records above): the segments log, per pixel
+ * and in list order, the alpha and depth of every Gaussian their warps evaluate (8 bytes each,
+ * and each step's Gaussian colour), and the last segment of a tile replays the log with the
+ * walk's own K-buffer and tail steps, so the operations and their order are those of the serial
+ * walk: images bit-identical to the default path.  The logs share one pool of `log_bytes`
+ * (0 = 8 GiB; about 2.2 KB per list entry of a split tile); a tile whose segments do
+ * not fit it is blended whole.  The share set by fhtgs_context_set_blend_split applies. */
+fhtgs_status fhtgs_context_set_blend_split_exact(fhtgs_context ctx, int32_t exact, int64_t log_bytes);
 /* The last frame's split blend: tiles split, segments blended, tiles blended whole after a record
  * overflow, and the most records one pixel of a segment produced.  Waits for the context's last
  * frame. */

@@ -197,3 +197,79 @@ def test_split_in_a_batch_of_mixed_views():
     for i, (a, b) in enumerate(zip(*out)):
         m = max_abs(a.cpu().numpy(), b.cpu().numpy())
         assert m <= 1e-4, f"view {i}: max-abs {m}"
+
+
+# ---- the exact split: fragment logs replayed in list order, images bit-identical ----
+
+def render_exact(gt, views, K=8, share=0.1, log_bytes=0, view_foveation=None, st_kw=None, **kw):
+    st = [F.settings_from_view(v, K=K, active_sh_bases=16, **(st_kw or {})) for v in views]
+    r = F.Renderer(DEV)
+    try:
+        r.set_blend_split(share, 0, exact=True, log_bytes=log_bytes)
+        imgs = [x.clone() for x in r.render(*gt, st, view_foveation=view_foveation, **kw)]
+        return imgs, r.blend_split_stats()
+    finally:
+        r.close()
+
+
+@pytest.mark.parametrize("K", [1, 8, 32])
+@pytest.mark.parametrize("fast_math", [True, False])
+def test_exact_split_is_bit_identical(stereo, K, fast_math):
+    _, gt, views = stereo
+    exact = render(gt, views, K=K, fast_math=fast_math)
+    split, stats = render_exact(gt, views, K=K, fast_math=fast_math)
+    assert stats["split_tiles"] > 0 and stats["segments"] > stats["split_tiles"]
+    for a, b in zip(exact, split):
+        assert torch.equal(a, b), f"K={K}: {int((a != b).sum())} values differ, max {float((a - b).abs().max()):.3g}"
+
+
+@pytest.mark.parametrize("case", ["blur", "sh_background", "rings", "aaa"])
+def test_exact_split_other_paths(stereo, case):
+    _, gt, views = stereo
+    kw, st_kw, vf = {}, {}, None
+    if case == "blur":
+        kw = dict(blur_periphery=True)
+    elif case == "aaa":
+        kw = dict(aaa_mode=True)
+    elif case == "rings":
+        vf = [("rings", 0.3, 0.6)] * 2
+    elif case == "sh_background":
+        st_kw = dict(background=F.BackgroundModel.SH, background_data=scene.sh_background(3))
+    st = [F.settings_from_view(v, K=8, active_sh_bases=16, **st_kw) for v in views]
+    r = F.Renderer(DEV)
+    exact = [x.clone() for x in r.render(*gt, st, view_foveation=vf, **kw)]
+    r.close()
+    split, stats = render_exact(gt, views, view_foveation=vf, st_kw=st_kw, **kw)
+    assert stats["split_tiles"] > 0
+    for a, b in zip(exact, split):
+        assert torch.equal(a, b)
+
+
+def test_exact_split_small_log_pool_leaves_tiles_whole(stereo):
+    _, gt, views = stereo
+    exact = render(gt, views)
+    big, s_big = render_exact(gt, views)
+    small, s_small = render_exact(gt, views, log_bytes=1 << 20)
+    assert s_small["split_tiles"] < s_big["split_tiles"]
+    for a, b, c in zip(exact, big, small):
+        assert torch.equal(a, b) and torch.equal(a, c)
+
+
+def test_exact_split_batch_and_graph():
+    g = scene.make_gaussians(150_000, 3, seed=43)
+    views = scene.make_batched_views(8, seed=7, radius=(3.0, 6.0),
+                                     resolutions=((320, 240), (640, 480), (272, 400), (800, 720)))
+    gt = F.gaussians_to_torch(g, DEV)
+    vf = ["none", ("rings", 0.15, 0.4), None, "none", ("rings", 0.3, 0.6), None, "none", None]
+    st = [F.settings_from_view(v, K=8, active_sh_bases=16) for v in views]
+    r = F.Renderer(DEV)
+    exact = [x.clone() for x in r.render(*gt, st, view_foveation=vf)]
+    r.set_blend_split(0.1, 0, exact=True)
+    split = [x.clone() for x in r.render(*gt, st, view_foveation=vf)]
+    assert r.blend_split_stats()["split_tiles"] > 0
+    graph = r.capture(*gt, st, view_foveation=vf, capacity_headroom=2.0)
+    replay = graph.launch(sync=True)
+    for a, b, c in zip(exact, split, replay):
+        assert torch.equal(a, b) and torch.equal(a, c)
+    graph.close()
+    r.close()
