@@ -146,6 +146,9 @@ def test_split_arguments_are_checked():
     for share, rec in ((0.01, 0), (9.0, 0), (-1.0, 0), (0.5, -1), (0.5, 257)):
         with pytest.raises(_lib.FhtgsError):
             r.set_blend_split(share, rec)
+    for log_bytes in (1000, -1, 65 << 30):
+        with pytest.raises(_lib.FhtgsError):
+            r.set_blend_split(0.5, 0, exact=True, log_bytes=log_bytes)
     r.set_blend_split(0.0, 0)
     r.close()
 
