@@ -109,3 +109,40 @@ def test_ties_keep_list_order():
              (np.float32(2.0), np.array([0, 0.1, 0, 0.5], np.float32)),
              (np.float32(1.0), np.array([0, 0, 0.1, 0.5], np.float32))]
     assert serial(frags, 2)[0] == split(frags, 2, [1])[0] == split(frags, 2, [2])[0]
+
+
+def exact_split(frags, K, cuts):
+    """The exact split: each segment logs its pairs (alpha, or -1 where the pair is no fragment;
+    depth) without a K-buffer, and the merge replays the logs of all segments in order with the
+    walk's own steps."""
+    log = []
+    for p in np.split(np.arange(len(frags)), cuts):
+        for i in p:
+            depth, pm = frags[i]
+            a = pm[3] if not pm[3] < MIN_ALPHA else np.float32(-1)
+            log.append((depth, a, pm))
+    core = [(BIG, 0)] * K
+    tail, T = np.zeros(4, np.float32), np.float32(1)
+    for depth, a, pm in log:
+        if a < 0:
+            continue
+        if a >= MIN_CORE:
+            ev = insert(core, depth, pack(pm))
+            if ev is not None:
+                pm = unpack(ev[1])
+        tail = tail + pm
+        T = T * (np.float32(1) - pm[3])
+    return core, tail, T
+
+
+@pytest.mark.parametrize("K", [1, 8, 32])
+def test_exact_split_replay_is_the_serial_walk(K):
+    rng = np.random.default_rng(100 + K)
+    for trial in range(10):
+        n = int(rng.integers(1, 300))
+        frags = stream(rng, n, bool(trial % 2))
+        cuts = sorted(int(c) for c in rng.integers(0, n + 1, int(rng.integers(1, 8))))
+        c0, t0, T0 = serial(frags, K)
+        c1, t1, T1 = exact_split(frags, K, cuts)
+        assert c0 == c1
+        assert np.array_equal(t0, t1) and T0 == T1  # same operations in the same order: bit for bit
