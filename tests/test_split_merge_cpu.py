@@ -4,7 +4,8 @@ contiguous segments, each walked from an empty K-buffer that records the fragmen
 then merged by replaying the records in order from the first segment's state.
 
 The K-buffer contents must agree exactly (same insertions and evictions, so the same RGBA8
-colours); the tail sum and its transmittance agree to float32 rounding.
+colours); the tail sum and its transmittance agree to float32 rounding.  The exact split (every
+segment logs its pairs, the merge replays all logs in order) must agree bit for bit.
 """
 import numpy as np
 import pytest
