@@ -415,6 +415,11 @@ def run_ours(a, world, rank, local):
     sm_clock = (clk or {}).get("sm_mhz") or 1965.0
     peak_fp32 = torch.cuda.get_device_properties(dev).multi_processor_count * FP32_LANES_PER_SM * 2 * sm_clock * 1e6 / 1e12
     achieved = pairs * FLOP_PER_PAIR / (blend_ms / 1000.0) / 1e12
+    if split is not None and split.get("stage_ms"):  # the same work over the split blend's time
+        split_achieved = pairs * FLOP_PER_PAIR / (split["stage_ms"]["blend"] / 1000.0) / 1e12
+        split["roofline"] = {"achieved": round(split_achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
+                             "frac": round(split_achieved / peak_fp32, 4), "kernel_ms": split["stage_ms"]["blend"],
+                             "work": "the default path's reference pair evaluations (see roofline)"}
 
     # ---- e2e through the public drop-in call with host buffers ----
     # Every step: the per-frame inputs (camera matrices, masks, tables; gaze is a host value)
