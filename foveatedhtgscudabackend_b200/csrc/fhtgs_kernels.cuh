@@ -1708,23 +1708,17 @@ struct BlendSmem {
     uint8_t (*list)[256];
 };
 
-// Renders one 16x16 work item with the whole 256-thread block: CLS 0 a full-resolution tile with
-// its 8 warps (each RW x 32/RW pixels: 8 x 4 laid out 2 x 4, 16 x 2 stacked, or 4 x 8 laid out
-// 4 x 2); CLS 1 a periphery tile sampled at stride 2 with warps 0-1 (each min(RW, 8) wide); CLS 2
-// a ring-mode quarter tile sampled at stride 4 with lanes 0-15 of warp 0.  The Gaussians of the
-// tile's list are staged in shared memory 256 at a time; each thread culls one of them against
-// the warp rectangles, and every warp then walks only its own compacted list, in list order.
-// The warp shape only changes which pairs are culled (pairs that cannot pass the alpha test),
-// never a pixel's arithmetic.  The tile layout is a compile-time constant of each class.
-// A segment of a split tile's list (SEG instantiation only).  mode 0: the whole list, resolved
-// as usual (a split tile blended whole); mode 1: the first segment, whose K-buffer, tail and
-// transmittance go to its scratch; mode 2: a later segment, walked from an empty K-buffer: every
-// fragment that enters it is recorded (depth, premultiplied colour) instead of being blended,
-// and the tail holds only the fragments that never entered it.
+// A segment of a split tile's list (SEG instantiations only).  SEG 1, the records mode: mode 0,
+// the whole list, resolved as usual (a split tile blended whole); mode 1, the first segment, whose
+// K-buffer, tail and transmittance go to its scratch; mode 2, a later segment, walked from an
+// empty K-buffer: every fragment that enters it is recorded (depth, premultiplied colour) instead
+// of being blended, and the tail holds only the fragments that never entered it.  SEG 3, the exact
+// split: the segment is walked without a K-buffer and every pair is logged (`recs` = the steps a
+// warp can take, the log's stride).
 struct SegWalk {
     uint32_t s, S;
     int mode;
-    int recs;  // records kept per pixel (mode 2)
+    int recs;  // SEG 1 mode 2: records kept per pixel; SEG 3: the log's stride in steps
     char* scratch;
 };
 
@@ -1757,6 +1751,14 @@ __device__ __forceinline__ void blend_resolve(const FrameParams& fp, const ViewP
               __saturatef(rgb.z));
 }
 
+// Renders one 16x16 work item with the whole 256-thread block: CLS 0 a full-resolution tile with
+// its 8 warps (each RW x 32/RW pixels: 8 x 4 laid out 2 x 4, 16 x 2 stacked, or 4 x 8 laid out
+// 4 x 2); CLS 1 a periphery tile sampled at stride 2 with warps 0-1 (each min(RW, 8) wide); CLS 2
+// a ring-mode quarter tile sampled at stride 4 with lanes 0-15 of warp 0.  The Gaussians of the
+// tile's list are staged in shared memory 256 at a time; each thread culls one of them against
+// the warp rectangles, and every warp then walks only its own compacted list, in list order.
+// The warp shape only changes which pairs are culled (pairs that cannot pass the alpha test),
+// never a pixel's arithmetic.  The tile layout is a compile-time constant of each class.
 template <int K, int RW, int CLS, int SEG = 0>
 __device__ __forceinline__ void blend_tile(const FrameParams& fp, const FrameBuffers& fb, uint32_t packed,
                                         const BlendSmem& sm, const SegWalk sw = SegWalk{0u, 1u, 0, 0, nullptr}) {
