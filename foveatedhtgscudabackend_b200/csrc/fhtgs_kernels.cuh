@@ -1695,9 +1695,8 @@ __device__ __forceinline__ bool conic_meets_rect(const Conic& q, float ax0, floa
     return !(m > 0.0f);
 }
 
-// One block renders one 16x16 area.  LOWRES: 64 threads sample it at stride 2 (periphery);
-// otherwise 256 threads render it at full resolution (fovea / blended).  Warp w covers an
-// 8-wide, 4-high block of samples.
+// Shared memory of a blend block: one batch of 256 staged Gaussian records (the three VPMT rows
+// and rgba), each Gaussian's warp-culling mask, and each warp's compacted list of batch positions.
 
 struct BlendSmem {
     float4* p1;
